@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark: time to solve the multi-RHS Wilson-Dirac system to an FP64 true residual
+of 1e-10, mixed-precision (BF16 storage, FP32 arithmetic, FP64 reliable updates) vs the
+plain FP64 BiCGStab on the same GPU and fields, plus the dslash roofline fraction.
+
+Workload: 24^3 x 48 lattice, SU(3), N_rhs = 12, kappa = 0.124, smoothed links
+U = exp(i 0.3 H), unit complex Gaussian sources, antiperiodic in t.  One step = one
+qcuInvert of the 12 right-hand sides.  Multi-GPU: independent replicas (one system per
+GPU), max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-solve at 1e-10 FP64 residual vs plain BiCGStab; dslash % of roofline"
+L = (24, 24, 24, 48)
+NC, M = 3, 12
+KAPPA = 0.124
+EPS = 0.3
+TOL = 1e-10
+T_BOUNDARY = -1.0
+MAX_ITER = 20000
+SEED_GAUGE, SEED_SRC = 2024, 7
+WORKLOAD = "24^3x48 SU(3) Wilson-Dirac, N_rhs=12, kappa=0.124, smoothed links eps=0.3, " \
+           "antiperiodic t, BiCGStab to FP64 true residual 1e-10"
+# Plain FP64 BiCGStab iterations this system needs (measured with this benchmark's
+# plain leg on a B200); the CPU reference leg multiplies its per-iteration time by it.
+PLAIN_ITERS = None
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def hop_bytes(vh, nc, m, s):
+    # algorithmic bytes of one half-lattice hop: 8 links + input and output spinor, once each
+    return vh * (8 * nc * nc * 2 * s + 2 * 4 * nc * m * 2 * s)
+
+
+def hop_flops(vh, nc, m):
+    return vh * m * (128 * nc * nc + 56 * nc)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_fields(rank):
+    """The benchmark's fields, generated on the host with torch's seeded CPU generator
+    (identical for both legs): gauge [4][2][Vh][3][3] and sources [12][2][Vh][4][3]."""
+    import torch
+    from qcu_mrhs_b200 import fields as F
+    torch.set_num_threads(os.cpu_count() or 1)
+    gauge = F.gauge_field_torch(L, NC, SEED_GAUGE + rank, kind="smooth", eps=EPS, device="cpu")
+    src = F.gaussian_fermions_torch(L, NC, M, SEED_SRC + rank, device="cpu")
+    return gauge, src
+
+
+def run_reference(args, world, rank):
+    """CPU reference leg: the FP64 policy-1 Schur BiCGStab of the CPU restatement
+    (the reference has no CPU implementation of its own), all host threads."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from qcu_mrhs_b200 import fields as F
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    gauge, b = make_fields(0)
+    gauge = gauge.numpy()
+    b = b.numpy()
+    bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
+    del b
+    iters = PLAIN_ITERS or 1
+    # one step: setup + one BiCGStab iteration (bounded sample); per-iteration time
+    # from the difference of one- and two-iteration runs
+    def one(n_it):
+        t0 = time.perf_counter()
+        O.bicgstab(bm, gauge, L, KAPPA, n_it, TOL, t_sign=T_BOUNDARY)
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        one(1)
+    t1 = [one(1) for _ in range(args.steps)]
+    t2 = one(2)
+    t_iter = max(t2 - statistics.median(t1), 1e-9)
+    t_setup = max(statistics.median(t1) - t_iter, 0.0)
+    value = t_setup + t_iter * iters
+    line = {
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(t1) * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded smoothed SU(3) links, unit complex Gaussian sources",
+        "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} x (setup + 1 iteration) and 1 x (setup + 2 iterations) of the "
+                                   f"FP64 policy-1 BiCGStab on the full workload; time-to-solve extrapolated "
+                                   f"as setup + per-iteration time x {iters} iterations"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import qcu_mrhs_b200 as q
+    from qcu_mrhs_b200 import fields as F
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = q.lib()
+    vh = F.half_volume(L)
+
+    # ---- inputs (on the device; host copies for the end-to-end leg) ----
+    gauge, src = make_fields(rank)
+    d_gauge = torch.view_as_real(gauge).contiguous().cuda()
+    d_src = [torch.view_as_real(src[j]).contiguous().cuda() for j in range(M)]
+    d_x = [torch.empty_like(d_src[0]) for _ in range(M)]
+    del gauge, src
+
+    grid = q.QcuGrid((ctypes.c_int * 4)(1, 1, 1, 1))
+    param = q.QcuParam((ctypes.c_int * 4)(*L))
+    lib.initGridSize(ctypes.byref(grid), ctypes.byref(param), NC, M, q.DOUBLE, q.BF16)
+    q.check()
+    lib.loadQcuGauge(d_gauge.data_ptr(), q.DOUBLE)
+    lib.getDslash(0, 1.0 / (2 * KAPPA) - 4.0)
+    q.check()
+
+    def set_opts(solver, sloppy=q.BF16):
+        o = q.default_options()
+        o.solver = solver
+        o.sloppy_precision = sloppy
+        o.stop_true_residual = 1
+        o.t_boundary = T_BOUNDARY
+        o.check_interval = 16
+        q.check(lib.qcuSetSolverOptions(ctypes.byref(o)))
+
+    def solve(srcs, outs, max_iter=MAX_ITER):
+        for j in range(M):
+            lib.pushBackFermions(outs[j].data_ptr(), srcs[j].data_ptr())
+        lib.qcuInvert(max_iter, TOL)
+        st = q.status()
+        if st not in (q.SUCCESS,):
+            raise RuntimeError(f"qcuInvert failed: {q.last_error()}")
+        return q.solve_stats()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- mixed precision (the product path) ----
+    set_opts(q.SOLVER_MIXED)
+    for _ in range(args.warmup):
+        stats = solve(d_src, d_x)
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    it_mixed, rel_mixed = [], []
+    for _ in range(args.steps):
+        stats = solve(d_src, d_x)
+        it_mixed.append(stats.iterations)
+        rel_mixed.append(max(stats.true_residual[:M]))
+    ev1.record()
+    torch.cuda.synchronize()
+    t_mixed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps)
+    clk = clocks.stop()
+    reliable = stats.reliable_updates
+
+    # ---- plain FP64 BiCGStab (same fields, same GPU) ----
+    set_opts(q.SOLVER_FUSED)
+    try:
+        solve(d_src, d_x, max_iter=4)
+    except RuntimeError:
+        pass   # warm-up of the FP64 kernels (not converged by design)
+    barrier()
+    ev0.record()
+    stats_plain = solve(d_src, d_x)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    it_plain = stats_plain.iterations
+    rel_plain = max(stats_plain.true_residual[:M])
+
+    # ---- dslash roofline: BF16 hop on the gathered layout (dominant kernel of the solve) ----
+    hbm, peak_kind = peaks()
+    stream = torch.cuda.current_stream()
+    dev_stream = ctypes.c_void_p(stream.cuda_stream)
+    roof = {}
+    for name, prec, dt in (("bf16", q.BF16, torch.bfloat16), ("f64", q.DOUBLE, torch.float64)):
+        s = q.PREC_BYTES[prec]
+        g_l = d_gauge.to(dt)
+        a = torch.randn((vh, 4, NC, M, 2), device="cuda").to(dt)
+        out = torch.empty_like(a)
+        Lc = q.lattice(L)
+        for _ in range(3):
+            q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
+                                      prec, dev_stream))
+        reps = 20
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(reps):
+            q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, i & 1, 0,
+                                      T_BOUNDARY, prec, dev_stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dur = e0.elapsed_time(e1) / 1e3 / reps
+        byts = hop_bytes(vh, NC, M, s)
+        roof[name] = {"bound": "hbm", "achieved": byts / dur / 1e9, "peak": hbm, "unit": "GB/s",
+                      "frac": byts / dur / 1e9 / hbm, "traffic": None, "launch_us": dur * 1e6,
+                      "algorithmic_bytes": byts, "gflops": hop_flops(vh, NC, M) / dur / 1e9,
+                      "peak_kind": f"{peak_kind} HBM copy bandwidth"}
+        del g_l, a, out
+
+    # ---- end to end through the C ABI with host buffers ----
+    h_gauge = torch.empty(d_gauge.shape, dtype=d_gauge.dtype, pin_memory=True)
+    h_gauge.copy_(d_gauge)
+    h_src = [torch.empty(d_src[0].shape, dtype=torch.float64, pin_memory=True) for _ in range(M)]
+    for j in range(M):
+        h_src[j].copy_(d_src[j])
+    h_x = [torch.empty_like(h_src[0]) for _ in range(M)]
+    set_opts(q.SOLVER_MIXED)
+    barrier()
+    ev0.record()
+    for _ in range(args.steps):
+        d_gauge.copy_(h_gauge, non_blocking=True)
+        for j in range(M):
+            d_src[j].copy_(h_src[j], non_blocking=True)
+        torch.cuda.synchronize()
+        lib.loadQcuGauge(d_gauge.data_ptr(), q.DOUBLE)
+        q.check()
+        solve(d_src, d_x)
+        for j in range(M):
+            h_x[j].copy_(d_x[j], non_blocking=True)
+        torch.cuda.synchronize()
+    ev1.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps)
+    h2d = h_gauge.numel() * 8 + sum(h.numel() * 8 for h in h_src)
+    d2h = sum(h.numel() * 8 for h in h_x)
+
+    # kernels launched per mixed solve: setup + 12 per graphed iteration (7 BiCGStab + 5 gated
+    # reliable-update kernels) rounded up to the graph length + reconstruction/statistics
+    interval = 16
+    graphed = -(-it_mixed[-1] // interval) * interval
+    launches_per_solve = 4 + 9 + 12 * graphed + 1 + 4 + 4
+    gpu_launches = launches_per_solve * args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(d_gauge, d_src, it_plain)
+
+    lib.finalizeQcu()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "dtype_detail": "BF16 storage, FP32 arithmetic, FP64 reductions and reliable updates",
+            "data": "synthetic: seeded smoothed SU(3) links exp(i 0.3 H), unit complex Gaussian sources",
+            "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA,
+                       "tol": TOL, "l2": "inputs larger than L2 (each hop reads 478 MB in BF16, 1.9 GB in FP64)",
+                       "replicas": world},
+            "solves_per_s_all_ranks": world / t_mixed,
+            "mixed": {"iterations": it_mixed[-1], "reliable_updates": reliable, "true_residual_max": max(rel_mixed)},
+            "plain_fp64": {"value": t_plain, "unit": "s", "iterations": it_plain, "true_residual_max": rel_plain,
+                           "speedup_mixed_vs_plain": t_plain / t_mixed},
+            "roofline": roof["bf16"],
+            "roofline_fp64_hop": roof["f64"],
+            "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "clocks": clk,
+            "gpu_launches": gpu_launches,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(d_gauge, d_src, plain_iters):
+    """CPU restatement (FP64 policy-1 BiCGStab), all host threads, bounded sample:
+    setup + 1 and setup + 2 iterations on the same fields; time-to-solve extrapolated
+    with the GPU plain solve's iteration count."""
+    from oracle import oracle as O
+    from qcu_mrhs_b200 import fields as F
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    g = d_gauge.cpu().numpy()
+    gauge = np.ascontiguousarray(g[..., 0] + 1j * g[..., 1])
+    b = np.stack([s.cpu().numpy() for s in d_src])
+    b = b[..., 0] + 1j * b[..., 1]                      # [m][2][vh][4][nc]
+    bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
+    del b, g
+
+    def one(n_it):
+        t0 = time.perf_counter()
+        O.bicgstab(bm, gauge, L, KAPPA, n_it, TOL, t_sign=T_BOUNDARY)
+        return time.perf_counter() - t0
+    t1 = one(1)
+    t2 = one(2)
+    t_iter = max(t2 - t1, 1e-9)
+    t_setup = max(t1 - t_iter, 0.0)
+    return {"value": t_setup + t_iter * plain_iters, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"setup+1 and setup+2 iterations of the FP64 policy-1 BiCGStab on the full workload "
+                      f"({t1 + t2:.1f} s of CPU work); extrapolated to {plain_iters} iterations",
+            "per_iteration_s": t_iter}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/*
+ * qcu_b200.h -- extensions of the qcu.h interface in libqcu_b200.so.
+ *
+ * Three groups:
+ *   1. status reporting, solver options and solve statistics for the qcu.h entry
+ *      points (the reference reports errors by aborting and has no options);
+ *   2. device-level entry points on caller-owned device buffers, one per reference
+ *      operator on the hot path (each cites the reference interface it replaces);
+ *   3. precision codes.
+ * All functions return a status code (QCU_SUCCESS = 0) unless stated otherwise.
+ * `stream` arguments are cudaStream_t values passed as void* (NULL = legacy stream).
+ */
+#pragma once
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- precision codes (reference enum QcuPrecision: half, single, double, undefined;
+ *      its numeric values live in a header outside the reference tree) ---- */
+#define QCU_PRECISION_HALF 0
+#define QCU_PRECISION_SINGLE 1
+#define QCU_PRECISION_DOUBLE 2
+#define QCU_PRECISION_UNDEFINED 3
+#define QCU_PRECISION_BF16 4 /* extension: bfloat16 storage, fp32 arithmetic */
+
+/* reference qcu_helper_macro.h:7-11 */
+#define QCU_DSLASH_WILSON 0
+
+/* ---- status codes ---- */
+#define QCU_SUCCESS 0
+#define QCU_ERR_INVALID 1        /* bad argument (size, precision, pointer) */
+#define QCU_ERR_STATE 2          /* wrong call order (not initialised, queue not full, ...) */
+#define QCU_ERR_CUDA 3           /* CUDA runtime error */
+#define QCU_ERR_NOT_CONVERGED 4  /* solver hit max_iteration */
+#define QCU_ERR_BREAKDOWN 5      /* solver breakdown (rho, omega or <r0,v> vanished / not finite) */
+#define QCU_ERR_UNSUPPORTED 6    /* feature not available */
+#define QCU_ERR_ALLOC 7          /* device allocation failed */
+
+/* Status of the most recent qcu.h / qcu_b200.h call on this process. */
+int qcuGetLastStatus(void);
+/* Human-readable message for the most recent failure ("" after success). */
+const char *qcuGetLastError(void);
+
+/* ---- solver selection for qcuInvert ---- */
+#define QCU_SOLVER_REFERENCE 0 /* reference policy-1 BiCGStab, output precision, recursive residual */
+#define QCU_SOLVER_FUSED 1     /* same iteration, fused device-resident kernels, CUDA graph */
+#define QCU_SOLVER_MIXED 2     /* sloppy-precision inner BiCGStab with FP64 reliable updates */
+
+typedef struct {
+    int solver;              /* QCU_SOLVER_* (default QCU_SOLVER_FUSED) */
+    int sloppy_precision;    /* inner precision for QCU_SOLVER_MIXED (QCU_PRECISION_*) */
+    int stop_true_residual;  /* 1: stop on FP64 true residual ||b - M x|| / ||b|| (full system);
+                                0: reference rule, recursive Schur residual ||r_o|| / ||b'_o|| */
+    double reliable_delta;   /* MIXED: reliable update when ||r|| < delta * max ||r|| (0.1) */
+    double t_boundary;       /* +1 periodic in t (reference), -1 antiperiodic in t */
+    int check_interval;      /* iterations per captured graph between host checks (8) */
+    int freeze_converged;    /* 1: converged right-hand sides stop updating */
+    int max_restarts;        /* MIXED: cap on reliable updates (0 = unlimited) */
+} QcuSolverOptions;
+
+void qcuGetDefaultSolverOptions(QcuSolverOptions *opts);
+/* Applies to the next qcuInvert / mat_Qcu / start_dslash of the current context. */
+int qcuSetSolverOptions(const QcuSolverOptions *opts);
+
+#define QCU_MAX_RHS 64
+
+typedef struct {
+    int iterations;          /* BiCGStab iterations (sloppy iterations for MIXED) */
+    int reliable_updates;    /* MIXED only */
+    int status;              /* QCU_SUCCESS, QCU_ERR_NOT_CONVERGED or QCU_ERR_BREAKDOWN */
+    int m_rhs;
+    double true_residual[QCU_MAX_RHS];      /* ||b - M x|| / ||b|| per RHS, full system, FP64 */
+    double recursive_residual[QCU_MAX_RHS]; /* last recursive Schur residual ||r|| / ||b'|| */
+    double solve_seconds;    /* device time of the solve (gather..scatter), CUDA events */
+} QcuSolveStats;
+
+/* Statistics of the last qcuInvert on the current context. */
+int qcuGetSolveStats(QcuSolveStats *stats);
+
+/* ---- device-level entry points (caller-owned device buffers) ----
+ * Gathered multi-RHS layout, one parity: [Vh][4][Nc][m] complex.
+ * Gauge: [4][2][Vh][Nc][Nc] complex in the same precision as the spinors.
+ * L = {Lx, Ly, Lz, Lt}.  2 <= n_color <= 8, 1 <= m_rhs <= 64.
+ */
+
+/* Hop term out[parity] = D in[1 - parity] on gathered fields.
+ * Replaces qcu::Dslash::apply -- reference include/qcd/qcu_dslash.h:56-74,
+ * src/qcd/qcu_dslash_wilson.cu:36-59 (wmma) and src/qcd/qcu_wilson_dslash_simt.cu:68-89 (SIMT). */
+int qcuDslashMrhs(void *out, const void *in, const void *gauge, const int L[4], int n_color,
+                  int m_rhs, int parity, int dagger, double t_sign, int precision, void *stream);
+
+/* out = x + a * D in  (the hop with the xpay epilogue of src/solver/bicgstab.cu:141-189). */
+int qcuDslashMrhsXpay(void *out, const void *in, const void *gauge, const void *x, double a,
+                      const int L[4], int n_color, int m_rhs, int parity, int dagger, double t_sign,
+                      int precision, void *stream);
+
+/* Schur operator out_o = in_o - kappa^2 D_oe D_eo in_o; tmp is one half-lattice vector.
+ * Replaces fused_x_sub_Doe_Deo_x -- reference src/solver/bicgstab_solve.cu:27-70. */
+int qcuSchurMrhs(void *out, const void *in, void *tmp, const void *gauge, double kappa,
+                 const int L[4], int n_color, int m_rhs, double t_sign, int precision, void *stream);
+
+/* Gather m per-RHS single-parity fields (array of m DEVICE pointers given as a HOST array)
+ * into the gathered layout, converting precision; and the reverse.
+ * Replaces colorSpinorGather / colorSpinorScatter -- reference
+ * src/data_format/qcu_data_format_shift.cu:163-205. vh = sites of one parity. */
+int qcuGatherMrhs(void *dst, int dst_precision, void *const *src_ptrs, int src_precision,
+                  int64_t vh, int n_color, int m_rhs, void *stream);
+int qcuScatterMrhs(void *const *dst_ptrs, int dst_precision, const void *src, int src_precision,
+                   int64_t vh, int n_color, int m_rhs, void *stream);
+
+/* Precision conversion of n complex numbers.
+ * Replaces copyComplexVector_interface -- reference src/data_format/qcu_data_format_shift.cu:141-161. */
+int qcuCopyComplexVector(void *dst, int dst_precision, const void *src, int src_precision,
+                         int64_t n, void *stream);
+
+/* Multi-RHS BLAS on strided vectors (element i of RHS j at complex offset i*m + j; len
+ * complex elements per RHS).  Scalars a, b, c and results are DEVICE arrays of m complex
+ * doubles (double2), vectors are in `precision`.  Reductions accumulate in FP64.
+ * Replace reference src/qcu_blas/qcu_complex_dotc.cu:20-75, qcu_complex_norm.cu:20-57,
+ * qcu_complex_xsay.cu, qcu_complex_xpay.cu, qcu_complex_axpby.cu, qcu_complex_axpbypcz.cu. */
+int qcuMrhsDotc(void *res, const void *a, const void *b, int64_t len, int m, int precision,
+                void *stream);                                  /* res_j = sum conj(a) b */
+int qcuMrhsNorm(double *res, const void *a, int64_t len, int m, int precision,
+                void *stream);                                  /* res_j = sqrt(sum |a|^2) */
+int qcuMrhsXsay(void *res, const void *x, const void *a, const void *y, int64_t len, int m,
+                int precision, void *stream);                   /* res = x - a_j y */
+int qcuMrhsXpay(void *res, const void *x, const void *a, const void *y, int64_t len, int m,
+                int precision, void *stream);                   /* res = x + a_j y */
+int qcuMrhsAxpby(void *res, const void *a, const void *x, const void *b, const void *y,
+                 int64_t len, int m, int precision, void *stream); /* res = a_j x + b_j y */
+int qcuMrhsAxpbypcz(void *res, const void *a, const void *x, const void *b, const void *y,
+                    const void *c, const void *z, int64_t len, int m, int precision,
+                    void *stream);                              /* res = a_j x + b_j y + c_j z */
+/* m-length complex scalar arrays (double2): reference src/qcu_blas/qcu_elementwise_{div,mul,init}.cu */
+int qcuElementwiseDiv(void *res, const void *x, const void *y, int m, void *stream);
+int qcuElementwiseMul(void *res, const void *x, const void *y, int m, void *stream);
+int qcuElementwiseInit(void *res, double re, double im, int m, void *stream);
+
+/* Gauge reorder lexicographic [4][Lt][Lz][Ly][Lx][Nc][Nc] <-> even/odd, on a given lattice
+ * (gauge_eo_precondition without a context). */
+int qcuGaugeToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
+int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
+
+/* Device synchronisation helper for bindings that have no CUDA runtime of their own. */
+int qcuDeviceSynchronize(void);
+
+#ifdef __cplusplus
+}
+#endif

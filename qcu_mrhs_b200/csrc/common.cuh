@@ -1,0 +1,165 @@
+// common.cuh -- shared types for the B200 multi-RHS Wilson library.
+//
+// Precision codes follow the reference's QcuPrecision order (half, single, double,
+// undefined); the numeric values live in an external header that is not part of
+// the reference tree, so these are this library's choice.  BF16 is an extension.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/qcu_b200.h"
+
+namespace qcub {
+
+constexpr int kNs = 4;          // spin components
+constexpr int kNd = 4;          // space-time dimensions
+constexpr int kMaxColor = 8;    // largest N with a compiled kernel
+constexpr int kMaxRhs = 64;     // largest m (per call) supported by the kernels
+
+// Record an error for qcuGetLastStatus()/qcuGetLastError(); returns the status.
+int set_error(int status, const char* fmt, ...);
+void clear_error();
+
+#define QCUB_CUDA_CHECK(expr)                                                                 \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return ::qcub::set_error(QCU_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #expr,   \
+                                     cudaGetErrorString(_e));                                 \
+    } while (0)
+
+#define QCUB_CHECK_LAUNCH() QCUB_CUDA_CHECK(cudaGetLastError())
+
+// Lattice geometry of one process (single GPU: the whole lattice).
+struct Geom {
+    int L[4];     // Lx, Ly, Lz, Lt
+    int lxh;      // Lx / 2
+    int64_t vh;   // half volume
+};
+
+inline Geom make_geom(const int L[4]) {
+    Geom g;
+    for (int i = 0; i < 4; ++i) g.L[i] = L[i];
+    g.lxh = L[0] / 2;
+    g.vh = (int64_t)L[0] * L[1] * L[2] * L[3] / 2;
+    return g;
+}
+
+inline size_t prec_bytes(int prec) {  // bytes of one real number
+    switch (prec) {
+        case QCU_PRECISION_DOUBLE: return 8;
+        case QCU_PRECISION_SINGLE: return 4;
+        case QCU_PRECISION_HALF:
+        case QCU_PRECISION_BF16: return 2;
+        default: return 0;
+    }
+}
+
+inline bool prec_valid(int prec) { return prec_bytes(prec) != 0; }
+
+// ---------------- storage traits ----------------
+// S: scalar storage type; S2: complex storage pair; A: arithmetic type; A2 its pair.
+template <typename S> struct St;
+template <> struct St<double> {
+    using S2 = double2;
+    using A = double;
+    using A2 = double2;
+    __host__ __device__ static A2 ld(const S2& v) { return v; }
+    __host__ __device__ static S2 cv(A2 v) { return v; }
+};
+template <> struct St<float> {
+    using S2 = float2;
+    using A = float;
+    using A2 = float2;
+    __host__ __device__ static A2 ld(const S2& v) { return v; }
+    __host__ __device__ static S2 cv(A2 v) { return v; }
+};
+template <> struct St<__half> {
+    using S2 = __half2;
+    using A = float;
+    using A2 = float2;
+    __device__ static A2 ld(const S2& v) { return __half22float2(v); }
+    __device__ static S2 cv(A2 v) { return __float22half2_rn(v); }
+};
+template <> struct St<__nv_bfloat16> {
+    using S2 = __nv_bfloat162;
+    using A = float;
+    using A2 = float2;
+    __device__ static A2 ld(const S2& v) { return __bfloat1622float2(v); }
+    __device__ static S2 cv(A2 v) { return __float22bfloat162_rn(v); }
+};
+
+// conversion between any two storage pairs, via the wider arithmetic type
+template <typename D, typename S>
+__device__ __forceinline__ typename St<D>::S2 convert2(const typename St<S>::S2& v) {
+    auto a = St<S>::ld(v);
+    using DA2 = typename St<D>::A2;
+    DA2 d;
+    d.x = (typename St<D>::A)a.x;
+    d.y = (typename St<D>::A)a.y;
+    return St<D>::cv(d);
+}
+
+// ---------------- complex helpers ----------------
+template <typename T> struct C2;
+template <> struct C2<double> { using T2 = double2; };
+template <> struct C2<float> { using T2 = float2; };
+
+template <typename T2>
+__host__ __device__ __forceinline__ T2 mk2(decltype(T2::x) a, decltype(T2::x) b) {
+    T2 r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+
+// acc += u * v
+template <typename T2>
+__device__ __forceinline__ void cmac(T2& acc, const T2& u, const T2& v) {
+    acc.x = fma(u.x, v.x, acc.x);
+    acc.x = fma(-u.y, v.y, acc.x);
+    acc.y = fma(u.x, v.y, acc.y);
+    acc.y = fma(u.y, v.x, acc.y);
+}
+// acc += conj(u) * v
+template <typename T2>
+__device__ __forceinline__ void cmac_conj(T2& acc, const T2& u, const T2& v) {
+    acc.x = fma(u.x, v.x, acc.x);
+    acc.x = fma(u.y, v.y, acc.x);
+    acc.y = fma(u.x, v.y, acc.y);
+    acc.y = fma(-u.y, v.x, acc.y);
+}
+
+// Dispatch on storage precision code.
+template <typename F>
+int dispatch_prec(int prec, F&& f) {
+    switch (prec) {
+        case QCU_PRECISION_DOUBLE: return f(double{});
+        case QCU_PRECISION_SINGLE: return f(float{});
+        case QCU_PRECISION_HALF: return f(__half{});
+        case QCU_PRECISION_BF16: return f(__nv_bfloat16{});
+        default: return set_error(QCU_ERR_INVALID, "unsupported precision code %d", prec);
+    }
+}
+
+int sm_count();
+
+// Resident blocks per SM of `kernel` at `block` threads (cached per kernel and size).
+int blocks_per_sm(const void* kernel, int block, size_t smem = 0);
+
+// Grid for a grid-stride kernel: enough blocks for the work, at most one full wave.
+template <typename K>
+static int resident_grid(K kernel, int block, int64_t work_items, size_t smem = 0) {
+    const int per_sm = blocks_per_sm(reinterpret_cast<const void*>(kernel), block, smem);
+    const int64_t want = (work_items + block - 1) / block;
+    const int64_t cap = (int64_t)per_sm * sm_count();
+    return (int)(want < cap ? (want < 1 ? 1 : want) : cap);
+}
+
+}  // namespace qcub

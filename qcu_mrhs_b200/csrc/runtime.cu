@@ -1,0 +1,122 @@
+// runtime.cu -- error state, device properties, occupancy cache, reduction scratch,
+// hop dispatch.
+#include <cstdarg>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "dslash.h"
+#include "workspace.h"
+
+namespace qcub {
+
+// ---------------- error state ----------------
+static thread_local int g_status = QCU_SUCCESS;
+static thread_local char g_message[512] = "";
+
+int set_error(int status, const char* fmt, ...) {
+    g_status = status;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_message, sizeof(g_message), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+void clear_error() {
+    g_status = QCU_SUCCESS;
+    g_message[0] = '\0';
+}
+
+int last_status() { return g_status; }
+const char* last_message() { return g_message; }
+
+// ---------------- device properties ----------------
+static std::mutex g_mu;
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cached[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+            n = 1;
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
+int blocks_per_sm(const void* kernel, int block, size_t smem) {
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto key = std::make_pair(kernel, block * 65536 + (int)(smem / 16));
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    cache[key] = per_sm;
+    return per_sm;
+}
+
+// ---------------- scratch ----------------
+int scratch_alloc(Scratch* s) {
+    s->max_blocks = kScratchBlocks;
+    const size_t pbytes = sizeof(double2) * (size_t)kScratchBlocks * kMaxRedVals * kMaxRhs;
+    QCUB_CUDA_CHECK(cudaMalloc(&s->partials, pbytes));
+    QCUB_CUDA_CHECK(cudaMalloc(&s->counter, 256));
+    QCUB_CUDA_CHECK(cudaMemset(s->counter, 0, 256));
+    QCUB_CUDA_CHECK(cudaMalloc(&s->result, sizeof(double2) * kMaxRedVals * kMaxRhs));
+    return QCU_SUCCESS;
+}
+
+void scratch_free(Scratch* s) {
+    if (s->partials) cudaFree(s->partials);
+    if (s->counter) cudaFree(s->counter);
+    if (s->result) cudaFree(s->result);
+    *s = Scratch{};
+}
+
+int device_scratch(const Scratch** out) {
+    static Scratch per_dev[64];
+    int dev = 0;
+    QCUB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(QCU_ERR_INVALID, "device index %d", dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (per_dev[dev].partials == nullptr) {
+        int rc = scratch_alloc(&per_dev[dev]);
+        if (rc) return rc;
+    }
+    *out = &per_dev[dev];
+    return QCU_SUCCESS;
+}
+
+// ---------------- hop dispatch ----------------
+template <typename S>
+static int hop_nc(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st) {
+    switch (nc) {
+        case 2: return launch_hop<2, S>(p, dagger, epi, st);
+        case 3: return launch_hop<3, S>(p, dagger, epi, st);
+        case 4: return launch_hop<4, S>(p, dagger, epi, st);
+        case 5: return launch_hop<5, S>(p, dagger, epi, st);
+        case 6: return launch_hop<6, S>(p, dagger, epi, st);
+        case 7: return launch_hop<7, S>(p, dagger, epi, st);
+        case 8: return launch_hop<8, S>(p, dagger, epi, st);
+        default: return set_error(QCU_ERR_UNSUPPORTED, "n_color=%d (supported: 2..8)", nc);
+    }
+}
+
+int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
+    if (p.m < 1 || p.m > kMaxRhs) return set_error(QCU_ERR_INVALID, "m_rhs=%d outside [1, %d]", p.m, kMaxRhs);
+    if (p.g.L[0] % 2 || p.g.L[0] < 2 || p.g.L[1] < 1 || p.g.L[2] < 1 || p.g.L[3] < 1)
+        return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", p.g.L[0], p.g.L[1],
+                         p.g.L[2], p.g.L[3]);
+    return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st); });
+}
+
+}  // namespace qcub

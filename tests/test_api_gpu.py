@@ -1,0 +1,204 @@
+"""The qcu.h flow on the GPU, used the way the reference's callers use it
+(initGridSize -> loadQcuGauge -> getDslash -> pushBackFermions x m ->
+start_dslash | mat_Qcu | qcuInvert -> finalizeQcu), checked against the oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import qcu_mrhs_b200 as q
+from qcu_mrhs_b200 import fields as F
+from tests.helpers import empty_dev, from_dev, rel_err, sync, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def init(L, nc, m, in_prec=q.DOUBLE, dslash_prec=q.DOUBLE):
+    grid = q.QcuGrid((ctypes.c_int * 4)(1, 1, 1, 1))
+    param = q.QcuParam((ctypes.c_int * 4)(*L))
+    q.lib().initGridSize(ctypes.byref(grid), ctypes.byref(param), nc, m, in_prec, dslash_prec)
+    q.check()
+
+
+@pytest.fixture(autouse=True)
+def _finalize():
+    yield
+    q.lib().finalizeQcu()
+
+
+def _setup(L, nc, m, kappa, seed, in_prec=q.DOUBLE, dslash_prec=q.DOUBLE, kind="haar"):
+    init(L, nc, m, in_prec, dslash_prec)
+    gauge = F.gauge_field(L, nc, seed, kind=kind, eps=0.3)
+    dg = to_dev(gauge, in_prec)
+    q.lib().loadQcuGauge(dg.data_ptr(), in_prec)
+    q.check()
+    q.lib().getDslash(0, 1.0 / (2 * kappa) - 4.0)
+    q.check()
+    return gauge, dg
+
+
+@pytest.mark.parametrize("dagger", [0, 1])
+def test_start_dslash(oracle_lib, dagger):
+    L, nc, m = (8, 8, 8, 8), 3, 4
+    gauge, dg = _setup(L, nc, m, 0.1, 1)
+    vh = F.half_volume(L)
+    psi = F.gaussian_fermions(L, nc, m, 2, parities=1)[:, 0]
+    ins = [to_dev(psi[j]) for j in range(m)]
+    for parity in (0, 1):
+        outs = [empty_dev((vh, 4, nc)) for _ in range(m)]
+        for j in range(m):
+            q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+        q.lib().start_dslash(parity, dagger)
+        q.check()
+        got = np.stack([from_dev(o) for o in outs])
+        ref = F.from_mrhs(oracle_lib.hop(F.to_mrhs(psi), gauge, L, parity, bool(dagger)))
+        assert rel_err(got, ref) <= 1e-13
+
+
+@pytest.mark.parametrize("dagger", [0, 1])
+def test_mat_qcu(oracle_lib, dagger):
+    L, nc, m, kappa = (8, 4, 4, 8), 3, 3, 0.12
+    gauge, dg = _setup(L, nc, m, kappa, 3)
+    vh = F.half_volume(L)
+    psi = F.gaussian_fermions(L, nc, m, 4)
+    ins = [to_dev(psi[j]) for j in range(m)]
+    outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+    for j in range(m):
+        q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+    q.lib().mat_Qcu(dagger)
+    q.check()
+    got = np.stack([from_dev(o) for o in outs])
+    ref = oracle_lib.mat(psi, gauge, L, kappa, bool(dagger))
+    assert rel_err(got, ref) <= 1e-13
+
+
+def test_mat_qcu_half_precision_dslash(oracle_lib):
+    L, nc, m, kappa = (8, 4, 4, 4), 3, 2, 0.11
+    gauge, dg = _setup(L, nc, m, kappa, 5, dslash_prec=q.HALF)
+    vh = F.half_volume(L)
+    psi = F.gaussian_fermions(L, nc, m, 6)
+    ins = [to_dev(psi[j]) for j in range(m)]
+    outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+    for j in range(m):
+        q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+    q.lib().mat_Qcu(0)
+    q.check()
+    got = np.stack([from_dev(o) for o in outs])
+    assert rel_err(got, oracle_lib.mat(psi, gauge, L, kappa)) <= 3e-3
+
+
+def _invert(L, nc, m, kappa, tol, seed, opts=None, max_iter=2000, kind="haar", t_boundary=1.0):
+    gauge, dg = _setup(L, nc, m, kappa, seed, kind=kind)
+    o = q.default_options()
+    o.t_boundary = t_boundary
+    if opts:
+        for k, v in opts.items():
+            setattr(o, k, v)
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    vh = F.half_volume(L)
+    b = F.gaussian_fermions(L, nc, m, seed + 1)
+    ins = [to_dev(b[j]) for j in range(m)]
+    outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+    for j in range(m):
+        q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+    q.lib().qcuInvert(max_iter, tol)
+    st = q.status()
+    x = np.stack([from_dev(o) for o in outs])
+    return gauge, b, x, st, q.solve_stats()
+
+
+def test_invert_matches_oracle_reference_rule(oracle_lib):
+    """Config 1: 8^4, SU(3) Haar, m = 4, kappa = 0.10, antiperiodic t, tol 1e-10."""
+    L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 4, 0.10, 1e-10
+    gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 10, t_boundary=-1.0)
+    assert st == q.SUCCESS, q.last_error()
+    bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
+    xo, it, rr = oracle_lib.bicgstab(bm, gauge, L, kappa, 2000, tol, t_sign=-1.0)
+    assert abs(stats.iterations - it) <= 1
+    xref = np.stack([F.from_mrhs(xo[0]), F.from_mrhs(xo[1])], axis=1)
+    assert rel_err(x, xref) <= 1e-9
+    res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-3, atol=1e-14)
+    assert np.all(np.array(stats.recursive_residual[:m]) <= tol)
+
+
+def test_invert_true_residual_rule(oracle_lib):
+    L, nc, m, kappa, tol = (8, 4, 4, 8), 3, 3, 0.12, 1e-10
+    gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 12, opts={"stop_true_residual": 1},
+                                     kind="smooth")
+    assert st == q.SUCCESS, q.last_error()
+    res = oracle_lib.mat(x, gauge, L, kappa) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.all(true_rel <= 1.5 * tol)
+
+
+@pytest.mark.parametrize("sloppy", [q.SINGLE, q.HALF, q.BF16])
+def test_mixed_precision_reaches_fp64_true_residual(oracle_lib, sloppy):
+    L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 4, 0.124, 1e-10
+    gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 14, kind="smooth", t_boundary=-1.0,
+                                     opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy})
+    assert st == q.SUCCESS, q.last_error()
+    assert stats.reliable_updates >= 1
+    res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.all(true_rel <= tol)
+    assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-2, atol=1e-15)
+
+
+def test_invert_not_converged_status():
+    L, nc, m = (4, 4, 4, 4), 3, 2
+    gauge, b, x, st, stats = _invert(L, nc, m, 0.12, 1e-14, 16, max_iter=3)
+    assert st == q.ERR_NOT_CONVERGED
+    assert stats.iterations == 3
+    assert np.all(np.isfinite(x))
+
+
+def test_zero_source_rhs_gives_zero_solution(oracle_lib):
+    L, nc, m, kappa = (4, 4, 4, 4), 3, 3, 0.1
+    gauge, dg = _setup(L, nc, m, kappa, 18)
+    vh = F.half_volume(L)
+    b = F.gaussian_fermions(L, nc, m, 19)
+    b[1] = 0
+    ins = [to_dev(b[j]) for j in range(m)]
+    outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+    for j in range(m):
+        q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+    q.lib().qcuInvert(500, 1e-10)
+    assert q.status() == q.SUCCESS, q.last_error()
+    x = np.stack([from_dev(o) for o in outs])
+    assert np.all(x[1] == 0)
+    res = oracle_lib.mat(x, gauge, L, kappa) - b
+    assert np.linalg.norm(res[0]) / np.linalg.norm(b[0]) < 1e-9
+
+
+def test_queue_rules():
+    L, nc, m = (4, 4, 4, 4), 3, 2
+    _setup(L, nc, m, 0.1, 20)
+    d = empty_dev((2, F.half_volume(L), 4, nc))
+    q.lib().pushBackFermions(d.data_ptr(), d.data_ptr())
+    q.lib().start_dslash(0, 0)
+    assert q.status() == q.ERR_STATE          # queue not full
+    q.lib().pushBackFermions(d.data_ptr(), d.data_ptr())
+    q.lib().pushBackFermions(d.data_ptr(), d.data_ptr())
+    q.lib().pushBackFermions(d.data_ptr(), d.data_ptr())
+    assert q.status() == q.ERR_STATE          # queue full
+    q.lib().getDslash(1, 0.0)
+    assert q.status() == q.ERR_UNSUPPORTED    # only Wilson
+
+
+def test_gauge_eo_precondition_through_context(oracle_lib):
+    L, nc, m = (4, 2, 2, 6), 3, 1
+    init(L, nc, m)
+    V = 4 * 2 * 2 * 6
+    rng = np.random.default_rng(21)
+    lex = rng.standard_normal((4, V, nc, nc)) + 1j * rng.standard_normal((4, V, nc, nc))
+    dl = to_dev(lex)
+    de = empty_dev(lex.shape)
+    q.lib().gauge_eo_precondition(de.data_ptr(), dl.data_ptr(), q.DOUBLE)
+    q.check()
+    assert np.array_equal(from_dev(de), oracle_lib.gauge_to_eo(lex, L))
+    back = empty_dev(lex.shape)
+    q.lib().gauge_reverse_eo_precondition(back.data_ptr(), de.data_ptr(), q.DOUBLE)
+    q.check()
+    assert np.array_equal(from_dev(back), lex)

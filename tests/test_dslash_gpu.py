@@ -1,0 +1,130 @@
+"""Hop term on the GPU vs the CPU oracle, through the C ABI (qcuDslashMrhs & co.).
+
+Tolerances (relative Frobenius error of the whole output):
+  FP64 <= 1e-13 against the oracle on the same inputs;
+  FP32 / FP16 / BF16 against the oracle run on the same *rounded* inputs:
+  FP32 1e-6, FP16 2e-3, BF16 1.5e-2 (output rounding plus FP32 accumulation).
+"""
+import numpy as np
+import pytest
+
+import qcu_mrhs_b200 as q
+from qcu_mrhs_b200 import fields as F
+from tests.helpers import empty_dev, from_dev, rel_err, sync, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL = {q.DOUBLE: 1e-13, q.SINGLE: 1e-6, q.HALF: 2e-3, q.BF16: 1.5e-2}
+
+
+def _round(arr, prec):
+    """Round a complex array to the storage precision and back (numpy/torch on CPU)."""
+    import torch
+    if prec == q.DOUBLE:
+        return arr
+    dt = {q.SINGLE: torch.float32, q.HALF: torch.float16, q.BF16: torch.bfloat16}[prec]
+    a = np.ascontiguousarray(arr, dtype=np.complex128)
+    t = torch.from_numpy(a.view(np.float64).reshape(a.shape + (2,)).copy()).to(dt).to(torch.float64).numpy()
+    return t[..., 0] + 1j * t[..., 1]
+
+
+def _problem(L, nc, m, seed, kind="haar"):
+    gauge = F.gauge_field(L, nc, seed, kind=kind)
+    psi = F.gaussian_fermions(L, nc, m, seed + 1, parities=1)[:, 0]
+    return gauge, F.to_mrhs(psi)
+
+
+def _hop_gpu(inp, gauge, L, parity, dagger, t_sign, prec):
+    nc, m = inp.shape[2], inp.shape[3]
+    d_in, d_g = to_dev(inp, prec), to_dev(gauge, prec)
+    d_out = empty_dev(inp.shape, prec)
+    rc = q.lib().qcuDslashMrhs(d_out.data_ptr(), d_in.data_ptr(), d_g.data_ptr(), q.lattice(L), nc, m,
+                               parity, int(dagger), float(t_sign), prec, None)
+    q.check(rc)
+    sync()
+    return from_dev(d_out)
+
+
+@pytest.mark.parametrize("parity", [0, 1])
+@pytest.mark.parametrize("dagger", [False, True])
+@pytest.mark.parametrize("t_sign", [1.0, -1.0])
+def test_fp64_hop_config1(oracle_lib, parity, dagger, t_sign):
+    L, nc, m = (8, 8, 8, 8), 3, 4
+    gauge, inp = _problem(L, nc, m, 11)
+    ref = oracle_lib.hop(inp, gauge, L, parity, dagger, t_sign)
+    got = _hop_gpu(inp, gauge, L, parity, dagger, t_sign, q.DOUBLE)
+    assert rel_err(got, ref) <= TOL[q.DOUBLE]
+
+
+@pytest.mark.parametrize("nc", [2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("m", [1, 3, 12, 32])
+def test_fp64_hop_colours_and_rhs(oracle_lib, nc, m):
+    L = (4, 4, 2, 6)
+    gauge, inp = _problem(L, nc, m, 20 + nc)
+    for parity in (0, 1):
+        ref = oracle_lib.hop(inp, gauge, L, parity, False, -1.0)
+        got = _hop_gpu(inp, gauge, L, parity, False, -1.0, q.DOUBLE)
+        assert rel_err(got, ref) <= TOL[q.DOUBLE]
+
+
+@pytest.mark.parametrize("L", [(2, 2, 2, 2), (2, 4, 6, 2), (10, 2, 2, 4), (6, 6, 6, 6)])
+def test_fp64_hop_shapes(oracle_lib, L):
+    gauge, inp = _problem(L, 3, 5, 31)
+    for parity in (0, 1):
+        ref = oracle_lib.hop(inp, gauge, L, parity, True, -1.0)
+        got = _hop_gpu(inp, gauge, L, parity, True, -1.0, q.DOUBLE)
+        assert rel_err(got, ref) <= TOL[q.DOUBLE]
+
+
+def test_fp64_hop_max_rhs(oracle_lib):
+    L = (4, 2, 2, 4)
+    gauge, inp = _problem(L, 3, 64, 33)
+    ref = oracle_lib.hop(inp, gauge, L, 1, False, 1.0)
+    assert rel_err(_hop_gpu(inp, gauge, L, 1, False, 1.0, q.DOUBLE), ref) <= TOL[q.DOUBLE]
+
+
+@pytest.mark.parametrize("prec", [q.SINGLE, q.HALF, q.BF16])
+@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (8, 16)])
+def test_low_precision_hop(oracle_lib, prec, nc, m):
+    L = (8, 4, 4, 4)
+    gauge, inp = _problem(L, nc, m, 40 + nc)
+    gr, ir = _round(gauge, prec), _round(inp, prec)
+    for parity in (0, 1):
+        ref = oracle_lib.hop(ir, gr, L, parity, False, -1.0)
+        got = _hop_gpu(inp, gauge, L, parity, False, -1.0, prec)
+        assert rel_err(got, ref) <= TOL[prec]
+        # error against the unrounded FP64 oracle stays within a few storage ulps
+        ref64 = oracle_lib.hop(inp, gauge, L, parity, False, -1.0)
+        assert rel_err(got, ref64) <= 4 * TOL[prec]
+
+
+def test_xpay_and_schur_epilogues(oracle_lib):
+    L, nc, m = (4, 4, 4, 4), 3, 6
+    gauge, inp = _problem(L, nc, m, 50)
+    x = F.to_mrhs(F.gaussian_fermions(L, nc, m, 51, parities=1)[:, 0])
+    d_in, d_g, d_x = to_dev(inp), to_dev(gauge), to_dev(x)
+    d_out, d_tmp = empty_dev(inp.shape), empty_dev(inp.shape)
+    rc = q.lib().qcuDslashMrhsXpay(d_out.data_ptr(), d_in.data_ptr(), d_g.data_ptr(), d_x.data_ptr(), -0.37,
+                                   q.lattice(L), nc, m, 0, 0, -1.0, q.DOUBLE, None)
+    q.check(rc)
+    sync()
+    ref = x - 0.37 * oracle_lib.hop(inp, gauge, L, 0, False, -1.0)
+    assert rel_err(from_dev(d_out), ref) <= 1e-13
+    kappa = 0.11
+    rc = q.lib().qcuSchurMrhs(d_out.data_ptr(), d_in.data_ptr(), d_tmp.data_ptr(), d_g.data_ptr(), kappa,
+                              q.lattice(L), nc, m, -1.0, q.DOUBLE, None)
+    q.check(rc)
+    sync()
+    ref = oracle_lib.schur(inp, gauge, L, kappa, -1.0)
+    assert rel_err(from_dev(d_out), ref) <= 1e-13
+
+
+def test_hop_rejects_bad_arguments():
+    L = q.lattice((8, 8, 8, 8))
+    d = empty_dev((16,))
+    p = d.data_ptr()
+    assert q.lib().qcuDslashMrhs(p, p, p, L, 9, 4, 0, 0, 1.0, q.DOUBLE, None) == q.ERR_UNSUPPORTED
+    assert q.lib().qcuDslashMrhs(p, p, p, L, 3, 65, 0, 0, 1.0, q.DOUBLE, None) == q.ERR_INVALID
+    assert q.lib().qcuDslashMrhs(p, p, p, L, 3, 4, 2, 0, 1.0, q.DOUBLE, None) == q.ERR_INVALID
+    assert q.lib().qcuDslashMrhs(p, p, p, q.lattice((7, 8, 8, 8)), 3, 4, 0, 0, 1.0, q.DOUBLE, None) == q.ERR_INVALID
+    assert q.lib().qcuDslashMrhs(p, p, p, L, 3, 4, 0, 0, 1.0, q.UNDEFINED, None) == q.ERR_INVALID
