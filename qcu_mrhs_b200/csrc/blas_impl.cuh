@@ -191,7 +191,7 @@ bicg_p_kernel(typename St<S>::S2* __restrict__ p, const typename St<S>::S2* __re
 __device__ __forceinline__ bool mp_skip(const BicgScalars* sc) { return sc->done || !sc->gate; }
 
 // x64 += e / scale_j ; e = 0     (gated by a pending reliable update)
-__global__ void __launch_bounds__(kRedThreads)
+static __global__ void __launch_bounds__(kRedThreads)
 mp_accum_kernel(double2* __restrict__ x64, float2* __restrict__ e, const BicgScalars* __restrict__ sc,
                 int64_t n, int m) {
     if (mp_skip(sc)) return;
@@ -245,7 +245,7 @@ mp_load_kernel(typename St<S>::S2* __restrict__ rs, typename St<S>::S2* __restri
 
 // One block: decide convergence from the FP64 true residual and rescale.
 // init: first call (sets scale from ||r64|| without touching counters).
-__global__ void mp_update_kernel(BicgScalars* sc, int m, int init) {
+static __global__ void mp_update_kernel(BicgScalars* sc, int m, int init) {
     if (!init && mp_skip(sc)) return;
     __shared__ int all_conv;
     if (threadIdx.x == 0) all_conv = 1;
