@@ -134,6 +134,15 @@ int qcuMrhsAxpby(void *res, const void *a, const void *x, const void *b, const v
 int qcuMrhsAxpbypcz(void *res, const void *a, const void *x, const void *b, const void *y,
                     const void *c, const void *z, int64_t len, int m, int precision,
                     void *stream);                              /* res = a_j x + b_j y + c_j z */
+/* qcuMrhsDotc for callers that cannot allocate device memory (their device memory is
+ * owned by another allocator, or allocation is not allowed on their code path).  No
+ * counterpart in the reference.  Same arguments and result as qcuMrhsDotc; never calls
+ * cudaMalloc or cudaFree: its scratch is a fixed 1 MiB device array inside the library
+ * (held on every GPU that loads it until exit).  m <= 64, else QCU_ERR_INVALID.  The
+ * first call on a device looks up the array's address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+int qcuMrhsDotcNoAlloc(void *res, const void *a, const void *b, int64_t len, int m, int precision,
+                       void *stream);
 /* m-length complex scalar arrays (double2): reference src/qcu_blas/qcu_elementwise_{div,mul,init}.cu */
 int qcuElementwiseDiv(void *res, const void *x, const void *y, int m, void *stream);
 int qcuElementwiseMul(void *res, const void *x, const void *y, int m, void *stream);

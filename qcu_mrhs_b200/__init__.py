@@ -91,6 +91,7 @@ _SIGNATURES = {
     "qcuScatterMrhs": (_i, [ctypes.POINTER(_vp), _i, _vp, _i, _i64, _i, _i, _vp]),
     "qcuCopyComplexVector": (_i, [_vp, _i, _vp, _i, _i64, _vp]),
     "qcuMrhsDotc": (_i, [_vp, _vp, _vp, _i64, _i, _i, _vp]),
+    "qcuMrhsDotcNoAlloc": (_i, [_vp, _vp, _vp, _i64, _i, _i, _vp]),
     "qcuMrhsNorm": (_i, [_vp, _vp, _i64, _i, _i, _vp]),
     "qcuMrhsXsay": (_i, [_vp, _vp, _vp, _vp, _i64, _i, _i, _vp]),
     "qcuMrhsXpay": (_i, [_vp, _vp, _vp, _vp, _i64, _i, _i, _vp]),
