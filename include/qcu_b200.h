@@ -153,6 +153,19 @@ int qcuElementwiseInit(void *res, double re, double im, int m, void *stream);
 int qcuGaugeToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
 int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
 
+/* Hop kernel selection for FP16/BF16 storage: tensor-core (tcgen05, TMEM accumulators)
+ * or SIMT FP32.  AUTO uses the tensor-core kernel where it covers the shape
+ * (2 <= n_color <= 8, m_rhs <= 32).  FP64 and FP32 always use the SIMT kernel. */
+#define QCU_HOP_AUTO 0
+#define QCU_HOP_SIMT 1
+#define QCU_HOP_TENSOR 2
+int qcuSetHopKernel(int kind);
+int qcuGetHopKernel(void);
+
+/* Nonzero if a kernel on the current device gave up a bounded wait (its results are then
+ * invalid); synchronises the device.  clear != 0 resets the flag. */
+int qcuGetKernelError(int clear);
+
 /* Device synchronisation helper for bindings that have no CUDA runtime of their own. */
 int qcuDeviceSynchronize(void);
 

@@ -23,6 +23,7 @@ PREC_BYTES = {HALF: 2, SINGLE: 4, DOUBLE: 8, BF16: 2}
 SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_UNSUPPORTED, ERR_ALLOC = range(8)
 
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED = 0, 1, 2
+HOP_AUTO, HOP_SIMT, HOP_TENSOR = 0, 1, 2
 MAX_RHS = 64
 
 
@@ -102,6 +103,9 @@ _SIGNATURES = {
     "qcuElementwiseInit": (_i, [_vp, _d, _d, _i, _vp]),
     "qcuGaugeToEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
     "qcuGaugeFromEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
+    "qcuSetHopKernel": (_i, [_i]),
+    "qcuGetHopKernel": (_i, []),
+    "qcuGetKernelError": (_i, [_i]),
     "qcuDeviceSynchronize": (_i, []),
 }
 

@@ -14,6 +14,9 @@
 namespace qcub {
 
 int last_status();
+int hop_kind();
+void set_hop_kind(int k);
+int* device_error_flag();
 const char* last_message();
 
 int DevBuf::ensure(size_t nbytes) {
@@ -572,6 +575,27 @@ int qcuGaugeFromEO(void* lex, const void* eo, const int L[4], int n_color, int p
     clear_error();
     if (!eo || !lex || !L) return set_error(QCU_ERR_INVALID, "null pointer");
     return gauge_reorder(lex, eo, L, n_color, precision, 0, static_cast<cudaStream_t>(stream));
+}
+
+int qcuSetHopKernel(int kind) {
+    clear_error();
+    if (kind != QCU_HOP_AUTO && kind != QCU_HOP_SIMT && kind != QCU_HOP_TENSOR)
+        return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
+    set_hop_kind(kind);
+    return QCU_SUCCESS;
+}
+
+int qcuGetHopKernel(void) { return hop_kind(); }
+
+int qcuGetKernelError(int clear) {
+    clear_error();
+    int* flag = device_error_flag();
+    if (!flag) return set_error(QCU_ERR_CUDA, "device error flag unavailable");
+    QCUB_CUDA_CHECK(cudaDeviceSynchronize());
+    int h = 0;
+    QCUB_CUDA_CHECK(cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear) QCUB_CUDA_CHECK(cudaMemset(flag, 0, sizeof(int)));
+    return h;
 }
 
 int qcuDeviceSynchronize(void) {

@@ -256,12 +256,15 @@ static __global__ void mp_update_kernel(BicgScalars* sc, int m, int init) {
         const bool conv = r2 <= sc->tol2 * sc->bfull2[j];
         if (conv) sc->active[j] = 0;
         if (!conv) atomicAnd(&all_conv, 0);
+        // scale so that the sloppy residual has unit RMS element (O(1) values keep FP16
+        // away from its subnormal range as the residual shrinks)
         const double rn = sqrt(r2);
-        const double snew = (rn > 0.0 && isfinite(rn)) ? 1.0 / rn : 1.0;
+        const double nrm = sqrt(sc->len_per_rhs);
+        const double snew = (rn > 0.0 && isfinite(rn)) ? nrm / rn : 1.0;
         sc->ratio[j] = snew / sc->scale[j];
         sc->scale[j] = snew;
-        sc->maxr[j] = 1.0;
-        sc->rnorm2[j] = 1.0;
+        sc->maxr[j] = nrm;
+        sc->rnorm2[j] = nrm * nrm;
         if (!isfinite(r2)) atomicAnd(&all_conv, 0);
     }
     __syncthreads();

@@ -36,11 +36,36 @@ void clear_error();
 
 #define QCUB_CHECK_LAUNCH() QCUB_CUDA_CHECK(cudaGetLastError())
 
+// Division by a fixed divisor d (1 <= d < 2^31) of n < 2^31 with one multiply-high:
+// q = (umulhi(n, m) + n) >> l with l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1
+// (round-up reciprocal method); (umulhi(n, m) + n) < 2^32 because both terms are < 2^31.
+struct FastDiv {
+    uint32_t d = 1, m = 1, l = 0;
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+        return (__umulhi(n, m) + n) >> l;
+#else
+        return (uint32_t)((((uint64_t)n * m) >> 32) + n) >> l;
+#endif
+    }
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    uint32_t l = 0;
+    while (l < 31 && (1ull << l) < d) ++l;
+    f.l = l;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d + 1) & 0xFFFFFFFFull);
+    return f;
+}
+
 // Lattice geometry of one process (single GPU: the whole lattice).
 struct Geom {
-    int L[4];     // Lx, Ly, Lz, Lt
-    int lxh;      // Lx / 2
-    int64_t vh;   // half volume
+    int L[4];      // Lx, Ly, Lz, Lt
+    int lxh;       // Lx / 2
+    int64_t vh;    // half volume (< 2^31: half-site indices are 32-bit in the kernels)
+    FastDiv dx, dy, dz;   // division by Lx/2, Ly, Lz
 };
 
 inline Geom make_geom(const int L[4]) {
@@ -48,7 +73,26 @@ inline Geom make_geom(const int L[4]) {
     for (int i = 0; i < 4; ++i) g.L[i] = L[i];
     g.lxh = L[0] / 2;
     g.vh = (int64_t)L[0] * L[1] * L[2] * L[3] / 2;
+    g.dx = make_fastdiv((uint32_t)(g.lxh > 0 ? g.lxh : 1));
+    g.dy = make_fastdiv((uint32_t)(L[1] > 0 ? L[1] : 1));
+    g.dz = make_fastdiv((uint32_t)(L[2] > 0 ? L[2] : 1));
     return g;
+}
+
+// half-site index -> (xh, y, z, t) with three multiply-high divisions
+struct SiteXYZT {
+    int xh, y, z, t;
+};
+__host__ __device__ __forceinline__ SiteXYZT site_coords(const Geom& g, uint32_t site) {
+    SiteXYZT c;
+    const uint32_t q1 = g.dx.div(site);
+    c.xh = (int)(site - q1 * (uint32_t)g.lxh);
+    const uint32_t q2 = g.dy.div(q1);
+    c.y = (int)(q1 - q2 * (uint32_t)g.L[1]);
+    const uint32_t q3 = g.dz.div(q2);
+    c.z = (int)(q2 - q3 * (uint32_t)g.L[2]);
+    c.t = (int)q3;
+    return c;
 }
 
 inline size_t prec_bytes(int prec) {  // bytes of one real number

@@ -141,11 +141,8 @@ __device__ __forceinline__ void hop_site(typename St<S>::A2 (&acc)[4][NC], const
     const int parity = p.parity;
     const int m = p.m;
     // half-site coordinates
-    int64_t q = site;
-    const int xh = (int)(q % lxh); q /= lxh;
-    const int y = (int)(q % Ly); q /= Ly;
-    const int z = (int)(q % Lz);
-    const int t = (int)(q / Lz);
+    const SiteXYZT sc = site_coords(p.g, (uint32_t)site);
+    const int xh = sc.xh, y = sc.y, z = sc.z, t = sc.t;
     const int xodd = (parity ^ (y + z + t)) & 1;  // full x = 2 xh + xodd
     const int64_t sy = lxh, sz = (int64_t)lxh * Ly, st = sz * Lz;
     const int64_t site_len = (int64_t)kNs * NC * m;
@@ -196,8 +193,16 @@ __device__ __forceinline__ void hop_site(typename St<S>::A2 (&acc)[4][NC], const
     }
 }
 
+// Minimum resident blocks per SM requested from the register allocator: FP64 at small N
+// otherwise takes ~190 registers (one block per SM, latency-bound); capping it at 128
+// doubles the warps in flight.  Large N keeps the compiler's choice (accumulators dominate).
+template <int NC, typename S>
+struct HopMinBlocks {
+    static constexpr int value = NC <= 4 ? (sizeof(S) == 8 ? 2 : 3) : 1;
+};
+
 template <int NC, typename S, bool DAG, int EPI>
-__global__ void __launch_bounds__(kRedThreads) hop_kernel(const HopParams p) {
+__global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_kernel(const HopParams p) {
     using S2 = typename St<S>::S2;
     using A = typename St<S>::A;
     using A2 = typename St<S>::A2;
@@ -215,8 +220,12 @@ __global__ void __launch_bounds__(kRedThreads) hop_kernel(const HopParams p) {
 #pragma unroll
     for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
 
-    for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += stride) {
-        const int64_t site = gi / m;
+    // block size and grid stride are multiples of m: the thread keeps RHS tid % m and
+    // walks sites without dividing
+    const int64_t site_stride = stride / m;
+    (void)total;
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / m + threadIdx.x / m; site < p.g.vh;
+         site += site_stride) {
         A2 acc[4][NC];
         hop_site<NC, S, DAG>(acc, p, site, rhs);
         const int64_t base = site * site_len + rhs;

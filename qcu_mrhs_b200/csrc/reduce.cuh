@@ -39,6 +39,7 @@ struct BicgScalars {
     int reliable;                       // reliable updates done
     int restart;                        // 1: the pending update also resets p and r0 (breakdown)
     double delta;                       // update when ||r_j|| < delta * maxr_j
+    double len_per_rhs;                 // complex elements per RHS of the sloppy vectors
     double scale[kMaxRhs];              // sloppy vectors hold scale_j * (FP64 quantity)
     double ratio[kMaxRhs];              // scale_new / scale_old of the last update
     double maxr[kMaxRhs];               // max sloppy ||r_j|| since the last update
@@ -185,26 +186,16 @@ __device__ inline void run_finisher(const RedArgs& ra, int m, const double2* sum
     }
 }
 
-// Block + grid reduction of NV double2 values per thread (thread's RHS = tid % m).
+// Grid stage of a reduction: every block publishes its per-RHS sums `bsum` (shared
+// memory, [NV][m], final for this block), the last block to arrive sums all blocks'
+// partials in a fixed order, writes the result and runs the finisher.
 // Must be called by every thread of the block, exactly once per launch.
 template <int NV>
-__device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs& ra) {
-    __shared__ double2 sh[NV * kRedThreads];
+__device__ inline void publish_and_finish(const double2* bsum, int m, const RedArgs& ra) {
     __shared__ bool s_last;
     const int tid = threadIdx.x;
     const int nb = blockDim.x;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) sh[k * nb + tid] = v[k];
-    __syncthreads();
-    for (int idx = tid; idx < NV * m; idx += nb) {
-        const int k = idx / m, j = idx - (idx / m) * m;
-        double2 s = make_double2(0.0, 0.0);
-        for (int i = j; i < nb; i += m) {
-            s.x += sh[k * nb + i].x;
-            s.y += sh[k * nb + i].y;
-        }
-        ra.partials[((size_t)blockIdx.x * NV + k) * m + j] = s;
-    }
+    for (int idx = tid; idx < NV * m; idx += nb) ra.partials[(size_t)blockIdx.x * NV * m + idx] = bsum[idx];
     __threadfence();
     __syncthreads();
     if (tid == 0) {
@@ -238,6 +229,30 @@ __device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs&
     if (tid == 0) *ra.counter = 0u;
     __syncthreads();
     if (ra.fin != FIN_NONE) run_finisher(ra, m, fin);
+}
+
+// Block + grid reduction of NV double2 values per thread (thread's RHS = tid % m).
+// Must be called by every thread of the block, exactly once per launch.
+template <int NV>
+__device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs& ra) {
+    __shared__ double2 sh[NV * kRedThreads];
+    __shared__ double2 bsum[NV * kMaxRhs];
+    const int tid = threadIdx.x;
+    const int nb = blockDim.x;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[k * nb + tid] = v[k];
+    __syncthreads();
+    for (int idx = tid; idx < NV * m; idx += nb) {
+        const int k = idx / m, j = idx - (idx / m) * m;
+        double2 s = make_double2(0.0, 0.0);
+        for (int i = j; i < nb; i += m) {
+            s.x += sh[k * nb + i].x;
+            s.y += sh[k * nb + i].y;
+        }
+        bsum[idx] = s;
+    }
+    __syncthreads();
+    publish_and_finish<NV>(bsum, m, ra);
 }
 
 // Block size for a kernel whose thread works on RHS tid % m: largest multiple of m <= cap.

@@ -96,6 +96,30 @@ int device_scratch(const Scratch** out) {
     return QCU_SUCCESS;
 }
 
+// ---------------- device error flag (bounded waits that gave up) ----------------
+int* device_error_flag() {
+    static int* per_dev[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (per_dev[dev] == nullptr) {
+        int* p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, sizeof(int));
+        per_dev[dev] = p;
+    }
+    return per_dev[dev];
+}
+
+// ---------------- hop kernel selection ----------------
+static int g_hop_kind = QCU_HOP_AUTO;
+
+int hop_kind() { return g_hop_kind; }
+void set_hop_kind(int k) { g_hop_kind = k; }
+
+bool hop_tc_supported(int nc, int m, int prec);
+int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
+
 // ---------------- hop dispatch ----------------
 template <typename S>
 static int hop_nc(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st) {
@@ -116,6 +140,9 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (p.g.L[0] % 2 || p.g.L[0] < 2 || p.g.L[1] < 1 || p.g.L[2] < 1 || p.g.L[3] < 1)
         return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", p.g.L[0], p.g.L[1],
                          p.g.L[2], p.g.L[3]);
+    const int kind = g_hop_kind;
+    if (kind != QCU_HOP_SIMT && hop_tc_supported(nc, p.m, prec))
+        return hop_tc_launch(p, nc, prec, dagger, epi, st);
     return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st); });
 }
 

@@ -96,6 +96,7 @@ int prepare_scalars(Context& c, BicgScalars* dsc, int max_iter, double tol, int 
     h.max_iter = max_iter;
     h.mixed = mixed;
     h.delta = c.opts.reliable_delta > 0 ? c.opts.reliable_delta : 0.1;
+    h.len_per_rhs = (double)c.half_len();
     for (int j = 0; j < c.m; ++j) {
         h.active[j] = 1;
         h.scale[j] = 1.0;

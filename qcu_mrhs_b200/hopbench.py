@@ -25,7 +25,7 @@ def hop_flops(vh, nc, m):
     return vh * m * (128 * nc * nc + 56 * nc)
 
 
-def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0):
+def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
     import torch
 
     import qcu_mrhs_b200 as q
@@ -40,6 +40,7 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0):
     st = torch.cuda.current_stream()
     sp = ctypes.c_void_p(st.cuda_stream)
     lib = q.lib()
+    q.check(lib.qcuSetHopKernel(kernel))
     bufs = (a, b)
     for i in range(warmup):
         q.check(lib.qcuDslashMrhs(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
@@ -54,7 +55,9 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0):
     torch.cuda.synchronize()
     dur = e0.elapsed_time(e1) / 1e3 / reps
     s = q.PREC_BYTES[prec]
-    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "launch_us": dur * 1e6,
+    q.check(lib.qcuSetHopKernel(0))
+    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "kernel": ["auto", "simt", "tcgen05"][kernel],
+            "launch_us": dur * 1e6,
             "GBps": hop_bytes(vh, nc, m, s) / dur / 1e9, "GFLOPs": hop_flops(vh, nc, m) / dur / 1e9,
             "algorithmic_bytes": hop_bytes(vh, nc, m, s)}
 
@@ -67,9 +70,13 @@ def main():
     ap.add_argument("--prec", nargs="+", default=["bf16", "f64"])
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--kernel", nargs="+", default=["auto"], choices=["auto", "simt", "tcgen05"])
     args = ap.parse_args()
-    for p in args.prec:
-        print(json.dumps(run(tuple(args.L), args.nc, args.m, p, args.reps, args.warmup)), flush=True)
+    for kname in args.kernel:
+        kern = {"auto": 0, "simt": 1, "tcgen05": 2}[kname]
+        for p in args.prec:
+            print(json.dumps(run(tuple(args.L), args.nc, args.m, p, args.reps, args.warmup, kernel=kern)),
+                  flush=True)
 
 
 if __name__ == "__main__":

@@ -83,19 +83,57 @@ def test_fp64_hop_max_rhs(oracle_lib):
     assert rel_err(_hop_gpu(inp, gauge, L, 1, False, 1.0, q.DOUBLE), ref) <= TOL[q.DOUBLE]
 
 
+@pytest.fixture
+def hop_kernel(request):
+    """Select the FP16/BF16 hop implementation for one test, restore AUTO afterwards."""
+    q.check(q.lib().qcuSetHopKernel(request.param))
+    yield request.param
+    q.lib().qcuSetHopKernel(q.HOP_AUTO)
+
+
+@pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT, q.HOP_TENSOR], indirect=True, ids=["simt", "tcgen05"])
 @pytest.mark.parametrize("prec", [q.SINGLE, q.HALF, q.BF16])
-@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (8, 16)])
-def test_low_precision_hop(oracle_lib, prec, nc, m):
+@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (8, 16), (2, 32), (6, 5)])
+def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
     L = (8, 4, 4, 4)
     gauge, inp = _problem(L, nc, m, 40 + nc)
     gr, ir = _round(gauge, prec), _round(inp, prec)
     for parity in (0, 1):
-        ref = oracle_lib.hop(ir, gr, L, parity, False, -1.0)
-        got = _hop_gpu(inp, gauge, L, parity, False, -1.0, prec)
-        assert rel_err(got, ref) <= TOL[prec]
-        # error against the unrounded FP64 oracle stays within a few storage ulps
-        ref64 = oracle_lib.hop(inp, gauge, L, parity, False, -1.0)
-        assert rel_err(got, ref64) <= 4 * TOL[prec]
+        for dagger in (False, True):
+            ref = oracle_lib.hop(ir, gr, L, parity, dagger, -1.0)
+            got = _hop_gpu(inp, gauge, L, parity, dagger, -1.0, prec)
+            assert rel_err(got, ref) <= TOL[prec]
+            # error against the unrounded FP64 oracle stays within a few storage ulps
+            ref64 = oracle_lib.hop(inp, gauge, L, parity, dagger, -1.0)
+            assert rel_err(got, ref64) <= 4 * TOL[prec]
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
+@pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR], indirect=True, ids=["tcgen05"])
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16])
+@pytest.mark.parametrize("L", [(2, 2, 2, 2), (6, 2, 4, 2), (4, 4, 4, 6)])
+def test_tensor_core_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel):
+    """Odd half volumes (last tile holds one site), tiny lattices, xpay and Schur epilogues."""
+    nc, m = 3, 7
+    gauge, inp = _problem(L, nc, m, 70)
+    gr, ir = _round(gauge, prec), _round(inp, prec)
+    x = F.to_mrhs(F.gaussian_fermions(L, nc, m, 71, parities=1)[:, 0])
+    xr = _round(x, prec)
+    d_in, d_g, d_x = to_dev(inp, prec), to_dev(gauge, prec), to_dev(x, prec)
+    d_out, d_tmp = empty_dev(inp.shape, prec), empty_dev(inp.shape, prec)
+    rc = q.lib().qcuDslashMrhsXpay(d_out.data_ptr(), d_in.data_ptr(), d_g.data_ptr(), d_x.data_ptr(), -0.37,
+                                   q.lattice(L), nc, m, 1, 0, 1.0, prec, None)
+    q.check(rc)
+    sync()
+    ref = xr - 0.37 * oracle_lib.hop(ir, gr, L, 1, False, 1.0)
+    assert rel_err(from_dev(d_out), ref) <= TOL[prec]
+    rc = q.lib().qcuSchurMrhs(d_out.data_ptr(), d_in.data_ptr(), d_tmp.data_ptr(), d_g.data_ptr(), 0.11,
+                              q.lattice(L), nc, m, -1.0, prec, None)
+    q.check(rc)
+    sync()
+    ref = oracle_lib.schur(ir, gr, L, 0.11, -1.0)
+    assert rel_err(from_dev(d_out), ref) <= 2 * TOL[prec]
+    assert q.lib().qcuGetKernelError(1) == 0
 
 
 def test_xpay_and_schur_epilogues(oracle_lib):
