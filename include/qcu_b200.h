@@ -154,8 +154,9 @@ int qcuGaugeToEO(void *eo, const void *lex, const int L[4], int n_color, int pre
 int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
 
 /* Hop kernel selection for FP16/BF16 storage: tensor-core (tcgen05, TMEM accumulators)
- * or SIMT FP32.  AUTO uses the tensor-core kernel where it covers the shape
- * (2 <= n_color <= 8, m_rhs <= 32).  FP64 and FP32 always use the SIMT kernel. */
+ * or SIMT FP32.  TENSOR uses the tensor-core kernel where it covers the shape
+ * (2 <= n_color <= 8, m_rhs <= 32); AUTO uses the SIMT kernel.  FP64 and FP32
+ * always use the SIMT kernel. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2

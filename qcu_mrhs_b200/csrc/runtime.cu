@@ -141,7 +141,7 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
         return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", p.g.L[0], p.g.L[1],
                          p.g.L[2], p.g.L[3]);
     const int kind = g_hop_kind;
-    if (kind != QCU_HOP_SIMT && hop_tc_supported(nc, p.m, prec))
+    if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec))
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
     return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st); });
 }
