@@ -153,15 +153,30 @@ int qcuElementwiseInit(void *res, double re, double im, int m, void *stream);
 int qcuGaugeToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
 int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
 
-/* Hop kernel selection for FP16/BF16 storage: tensor-core (tcgen05, TMEM accumulators)
- * or SIMT FP32.  TENSOR uses the tensor-core kernel where it covers the shape
- * (2 <= n_color <= 8, m_rhs <= 32); AUTO uses the SIMT kernel.  FP64 and FP32
- * always use the SIMT kernel. */
+/* Hop kernel selection.
+ *   SIMT     one thread per (site, RHS), all colours in registers;
+ *   SIMT_CS  one thread per (site, RHS, colour): fewer registers (FP64, large N),
+ *            needs n_color * m_rhs <= 256 (else SIMT);
+ *   TENSOR   FP16/BF16 storage on the tcgen05 tensor cores with TMEM accumulators and
+ *            bulk-copy (TMA) staged neighbour spinors, for 2 <= n_color <= 4 and
+ *            m_rhs <= 32 (else SIMT);
+ *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
+ *            (n_color, m_rhs, precision), else a static rule. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2
+#define QCU_HOP_SIMT_CS 3
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
+
+/* Autotuner: times every hop kernel that covers (n_color, m_rhs, precision) on a lattice
+ * L with synthetic fields (allocates and frees temporary device buffers), records the
+ * fastest for AUTO and, when the environment variable QCU_TUNE_CACHE names a file,
+ * appends "n_color m_rhs precision kind microseconds" to it (read back on first use).
+ * Returns the chosen QCU_HOP_* kind (>= 1) or a negative status. */
+int qcuTuneHop(const int L[4], int n_color, int m_rhs, int precision, void *stream);
+/* Recorded choice for AUTO (0 = none recorded). */
+int qcuGetTunedHop(int n_color, int m_rhs, int precision);
 
 /* Nonzero if a kernel on the current device gave up a bounded wait (its results are then
  * invalid); synchronises the device.  clear != 0 resets the flag. */

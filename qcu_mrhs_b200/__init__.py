@@ -23,7 +23,7 @@ PREC_BYTES = {HALF: 2, SINGLE: 4, DOUBLE: 8, BF16: 2}
 SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_UNSUPPORTED, ERR_ALLOC = range(8)
 
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED = 0, 1, 2
-HOP_AUTO, HOP_SIMT, HOP_TENSOR = 0, 1, 2
+HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS = 0, 1, 2, 3
 MAX_RHS = 64
 
 
@@ -106,6 +106,8 @@ _SIGNATURES = {
     "qcuSetHopKernel": (_i, [_i]),
     "qcuGetHopKernel": (_i, []),
     "qcuGetKernelError": (_i, [_i]),
+    "qcuTuneHop": (_i, [_ip, _i, _i, _i, _vp]),
+    "qcuGetTunedHop": (_i, [_i, _i, _i]),
     "qcuDeviceSynchronize": (_i, []),
 }
 

@@ -276,8 +276,177 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Colour-split variant: one thread per (half-site, RHS, output colour c).  The thread
+// projects the full neighbour spinor (the N threads of one (site, RHS) are adjacent
+// lanes and read the same addresses, which the load unit merges), applies row c of
+// the link (column c of its adjoint), and keeps only 4 complex accumulators.  This
+// trades more load/projection instructions for far fewer registers: it lifts
+// occupancy for FP64 and makes large N (6, 8) fit without spilling.
+// Block size and grid stride are multiples of N*m; thread tid works on
+// c = tid % N, RHS = (tid / N) % m.
+template <int NC, typename S, bool DAG, int EPI>
+__global__ void __launch_bounds__(kRedThreads) hop_kernel_cs(const HopParams p) {
+    using S2 = typename St<S>::S2;
+    using A = typename St<S>::A;
+    using A2 = typename St<S>::A2;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int SF = DAG ? 1 : -1;    // sign of gamma in the forward projector
+    constexpr int SB = DAG ? -1 : 1;    // ... in the backward projector
+    constexpr int N2 = NC * NC;
+    if (skip_launch(p.done, p.gate)) return;
+    const int m = p.m;
+    const int c = threadIdx.x % NC;
+    const int rhs = (threadIdx.x / NC) % m;
+    const int64_t per_site = (int64_t)NC * m;
+    const int64_t site_stride = ((int64_t)gridDim.x * blockDim.x) / per_site;
+    const int64_t site_len = (int64_t)kNs * NC * m;
+    const S2* __restrict__ in = static_cast<const S2*>(p.in);
+    const S2* __restrict__ gauge = static_cast<const S2*>(p.gauge);
+    S2* __restrict__ out = static_cast<S2*>(p.out);
+    const S2* __restrict__ xv = static_cast<const S2*>(p.x);
+    const S2* __restrict__ r0 = static_cast<const S2*>(p.r0);
+    const int lxh = p.g.lxh, Ly = p.g.L[1], Lz = p.g.L[2], Lt = p.g.L[3];
+    const int64_t vh = p.g.vh;
+    const int64_t sy = lxh, sz = (int64_t)lxh * Ly, st = sz * Lz;
+    const int parity = p.parity;
+    const S2* gf = gauge + (int64_t)parity * vh * N2;
+    const S2* gb = gauge + (int64_t)(1 - parity) * vh * N2;
+    const int64_t gmu = 2 * vh * N2;
+    double2 red[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / per_site + threadIdx.x / per_site; site < vh;
+         site += site_stride) {
+        const SiteXYZT sc = site_coords(p.g, (uint32_t)site);
+        const int xh = sc.xh, y = sc.y, z = sc.z, t = sc.t;
+        const int xodd = (parity ^ (y + z + t)) & 1;
+        A2 acc[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i] = mk2<A2>(0, 0);
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+            const int mu = h >> 1;
+            const bool fwd = (h & 1) == 0;
+            int64_t nb;
+            bool wrap = false;
+            if (mu == 0) {
+                nb = fwd ? site - xh + (xodd ? (xh + 1 == lxh ? 0 : xh + 1) : xh)
+                         : site - xh + (xodd ? xh : (xh == 0 ? lxh - 1 : xh - 1));
+            } else if (mu == 1) {
+                nb = fwd ? site + (y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy)
+                         : site + (y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
+            } else if (mu == 2) {
+                nb = fwd ? site + (z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz)
+                         : site + (z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
+            } else {
+                wrap = fwd ? (t + 1 == Lt) : (t == 0);
+                nb = fwd ? site + (wrap ? -(int64_t)(Lt - 1) * st : st)
+                         : site + (wrap ? (int64_t)(Lt - 1) * st : -st);
+            }
+            const A sg = (A)(fwd ? SF : SB);
+            const S2* psi = in + nb * site_len + rhs;
+            const S2* U = fwd ? gf + mu * gmu + site * N2 : gb + mu * gmu + nb * N2;
+            A2 w0 = mk2<A2>(0, 0), w1 = mk2<A2>(0, 0);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const A2 p0 = St<S>::ld(psi[(0 * NC + k) * m]);
+                const A2 p1 = St<S>::ld(psi[(1 * NC + k) * m]);
+                const A2 p2 = St<S>::ld(psi[(2 * NC + k) * m]);
+                const A2 p3 = St<S>::ld(psi[(3 * NC + k) * m]);
+                A2 h0, h1;
+                if (mu == 0) {
+                    h0 = mk2<A2>(p0.x - sg * p3.y, p0.y + sg * p3.x);
+                    h1 = mk2<A2>(p1.x - sg * p2.y, p1.y + sg * p2.x);
+                } else if (mu == 1) {
+                    h0 = mk2<A2>(p0.x - sg * p3.x, p0.y - sg * p3.y);
+                    h1 = mk2<A2>(p1.x + sg * p2.x, p1.y + sg * p2.y);
+                } else if (mu == 2) {
+                    h0 = mk2<A2>(p0.x - sg * p2.y, p0.y + sg * p2.x);
+                    h1 = mk2<A2>(p1.x + sg * p3.y, p1.y - sg * p3.x);
+                } else {
+                    h0 = mk2<A2>(p0.x + sg * p2.x, p0.y + sg * p2.y);
+                    h1 = mk2<A2>(p1.x + sg * p3.x, p1.y + sg * p3.y);
+                }
+                if (fwd) {
+                    const A2 u = St<S>::ld(U[c * NC + k]);
+                    cmac(w0, u, h0);
+                    cmac(w1, u, h1);
+                } else {
+                    const A2 u = St<S>::ld(U[k * NC + c]);
+                    cmac_conj(w0, u, h0);
+                    cmac_conj(w1, u, h1);
+                }
+            }
+            if (wrap) {
+                w0 = scale2(w0, (A)p.t_sign);
+                w1 = scale2(w1, (A)p.t_sign);
+            }
+            acc[0].x += w0.x; acc[0].y += w0.y;
+            acc[1].x += w1.x; acc[1].y += w1.y;
+            if (mu == 0) {
+                acc[2].x += sg * w1.y; acc[2].y -= sg * w1.x;
+                acc[3].x += sg * w0.y; acc[3].y -= sg * w0.x;
+            } else if (mu == 1) {
+                acc[2].x += sg * w1.x; acc[2].y += sg * w1.y;
+                acc[3].x -= sg * w0.x; acc[3].y -= sg * w0.y;
+            } else if (mu == 2) {
+                acc[2].x += sg * w0.y; acc[2].y -= sg * w0.x;
+                acc[3].x -= sg * w1.y; acc[3].y += sg * w1.x;
+            } else {
+                acc[2].x += sg * w0.x; acc[2].y += sg * w0.y;
+                acc[3].x += sg * w1.x; acc[3].y += sg * w1.y;
+            }
+        }
+        const int64_t base = site * site_len + rhs + (int64_t)c * m;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int64_t o = base + (int64_t)s * NC * m;
+            const A2 v = acc[s];
+            if (EPI == EPI_PLAIN) {
+                out[o] = St<S>::cv(v);
+            } else {
+                const A2 xx = St<S>::ld(xv[o]);
+                const A a = (A)p.a;
+                A2 res;
+                if (EPI == EPI_XPAY) {
+                    res = mk2<A2>(xx.x + a * v.x, xx.y + a * v.y);
+                } else if (EPI == EPI_RESID) {
+                    const A2 yy = St<S>::ld(r0[o]);
+                    res = mk2<A2>(yy.x - xx.x + a * v.x, yy.y - xx.y + a * v.y);
+                } else {
+                    res = mk2<A2>(xx.x - a * v.x, xx.y - a * v.y);
+                }
+                const S2 rs = St<S>::cv(res);
+                out[o] = rs;
+                if (NV > 0) {
+                    const A2 rr = St<S>::ld(rs);
+                    if (EPI == EPI_RESID) {
+                        red[0].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                    } else if (EPI == EPI_SCHUR_R0) {
+                        const A2 q = St<S>::ld(r0[o]);
+                        red[0].x += (double)q.x * rr.x + (double)q.y * rr.y;
+                        red[0].y += (double)q.x * rr.y - (double)q.y * rr.x;
+                    } else if (EPI == EPI_SCHUR_TS) {
+                        red[0].x += (double)rr.x * xx.x + (double)rr.y * xx.y;
+                        red[0].y += (double)rr.x * xx.y - (double)rr.y * xx.x;
+                        red[NV - 1].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (NV > 0) {
+        double2 rv[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        grid_reduce<NV>(rv, m, p.red, NC);
+    }
+}
+
 // Host launcher for one instantiation (defined in the per-precision .cu files).
 template <int NC, typename S>
-int launch_hop(const HopParams& p, bool dagger, int epi, cudaStream_t stream);
+int launch_hop(const HopParams& p, bool dagger, int epi, cudaStream_t stream, bool color_split);
 
 }  // namespace qcub

@@ -231,10 +231,11 @@ __device__ inline void publish_and_finish(const double2* bsum, int m, const RedA
     if (ra.fin != FIN_NONE) run_finisher(ra, m, fin);
 }
 
-// Block + grid reduction of NV double2 values per thread (thread's RHS = tid % m).
+// Block + grid reduction of NV double2 values per thread.  Thread tid works on RHS
+// (tid / g) % m (g = 1: tid % m; the colour-split hop has g = n_color).
 // Must be called by every thread of the block, exactly once per launch.
 template <int NV>
-__device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs& ra) {
+__device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs& ra, int g = 1) {
     __shared__ double2 sh[NV * kRedThreads];
     __shared__ double2 bsum[NV * kMaxRhs];
     const int tid = threadIdx.x;
@@ -245,10 +246,11 @@ __device__ inline void grid_reduce(const double2 (&v)[NV], int m, const RedArgs&
     for (int idx = tid; idx < NV * m; idx += nb) {
         const int k = idx / m, j = idx - (idx / m) * m;
         double2 s = make_double2(0.0, 0.0);
-        for (int i = j; i < nb; i += m) {
-            s.x += sh[k * nb + i].x;
-            s.y += sh[k * nb + i].y;
-        }
+        for (int base = j * g; base < nb; base += g * m)
+            for (int l = 0; l < g && base + l < nb; ++l) {
+                s.x += sh[k * nb + base + l].x;
+                s.y += sh[k * nb + base + l].y;
+            }
         bsum[idx] = s;
     }
     __syncthreads();

@@ -118,19 +118,24 @@ int hop_kind() { return g_hop_kind; }
 void set_hop_kind(int k) { g_hop_kind = k; }
 
 bool hop_tc_supported(int nc, int m, int prec);
+
+// Kernel used when the selection is AUTO: the tuned choice for (n_color, m, precision)
+// if one was recorded (qcuTuneHop / the tuning cache), else a static rule: colour-split
+// SIMT for FP64 and for N >= 5 (fewer registers), per-(site, RHS) SIMT otherwise.
+int auto_hop_kind(int nc, int m, int prec);
 int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 
 // ---------------- hop dispatch ----------------
 template <typename S>
-static int hop_nc(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st) {
+static int hop_nc(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st, bool cs) {
     switch (nc) {
-        case 2: return launch_hop<2, S>(p, dagger, epi, st);
-        case 3: return launch_hop<3, S>(p, dagger, epi, st);
-        case 4: return launch_hop<4, S>(p, dagger, epi, st);
-        case 5: return launch_hop<5, S>(p, dagger, epi, st);
-        case 6: return launch_hop<6, S>(p, dagger, epi, st);
-        case 7: return launch_hop<7, S>(p, dagger, epi, st);
-        case 8: return launch_hop<8, S>(p, dagger, epi, st);
+        case 2: return launch_hop<2, S>(p, dagger, epi, st, cs);
+        case 3: return launch_hop<3, S>(p, dagger, epi, st, cs);
+        case 4: return launch_hop<4, S>(p, dagger, epi, st, cs);
+        case 5: return launch_hop<5, S>(p, dagger, epi, st, cs);
+        case 6: return launch_hop<6, S>(p, dagger, epi, st, cs);
+        case 7: return launch_hop<7, S>(p, dagger, epi, st, cs);
+        case 8: return launch_hop<8, S>(p, dagger, epi, st, cs);
         default: return set_error(QCU_ERR_UNSUPPORTED, "n_color=%d (supported: 2..8)", nc);
     }
 }
@@ -140,10 +145,13 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (p.g.L[0] % 2 || p.g.L[0] < 2 || p.g.L[1] < 1 || p.g.L[2] < 1 || p.g.L[3] < 1)
         return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", p.g.L[0], p.g.L[1],
                          p.g.L[2], p.g.L[3]);
-    const int kind = g_hop_kind;
-    if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec))
+    int kind = g_hop_kind;
+    if (kind == QCU_HOP_AUTO) kind = auto_hop_kind(nc, p.m, prec);
+    if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec) &&
+        reinterpret_cast<uintptr_t>(p.in) % 16 == 0)
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
-    return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st); });
+    const bool cs = (kind == QCU_HOP_SIMT_CS) && nc * p.m <= kRedThreads;
+    return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st, cs); });
 }
 
 }  // namespace qcub

@@ -1,0 +1,173 @@
+// tune.cu -- hop-kernel autotuner: measures every kernel that covers a shape and records
+// the fastest for QCU_HOP_AUTO, optionally persisted in a plain-text cache file.
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "dslash.h"
+
+namespace qcub {
+
+bool hop_tc_supported(int nc, int m, int prec);
+void set_hop_kind(int k);
+int hop_kind();
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;   // (device, nc, m, prec) -> kind
+bool g_cache_loaded = false;
+
+int current_device() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+
+void load_cache_locked() {
+    if (g_cache_loaded) return;
+    g_cache_loaded = true;
+    const char* path = std::getenv("QCU_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    int nc, m, prec, kind;
+    double us;
+    const int dev = current_device();
+    while (std::fscanf(f, "%d %d %d %d %lf", &nc, &m, &prec, &kind, &us) == 5)
+        g_tuned[std::make_tuple(dev, nc, m, prec)] = kind;
+    std::fclose(f);
+}
+
+__global__ void fill_kernel(uint32_t* p, int64_t n, uint32_t seed) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x = (uint32_t)i * 2654435761u + seed;
+        x ^= x >> 13;
+        x *= 0x5bd1e995u;
+        x ^= x >> 15;
+        // small finite values in every storage format: exponent bits kept moderate
+        p[i] = x & 0x3C7F3C7Fu;
+    }
+}
+}  // namespace
+
+int auto_hop_kind(int nc, int m, int prec) {
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        load_cache_locked();
+        auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
+        if (it != g_tuned.end()) return it->second;
+    }
+    if (prec == QCU_PRECISION_DOUBLE || nc >= 5) return nc * m <= kRedThreads ? QCU_HOP_SIMT_CS : QCU_HOP_SIMT;
+    return QCU_HOP_SIMT;
+}
+
+int tuned_hop(int nc, int m, int prec) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    load_cache_locked();
+    auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
+    return it == g_tuned.end() ? 0 : it->second;
+}
+
+// Returns the fastest kind (>= 1) or a negative status.
+int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* best_us) {
+    if (!prec_valid(prec)) return -set_error(QCU_ERR_INVALID, "precision %d", prec);
+    const Geom g = make_geom(L);
+    const size_t rb = prec_bytes(prec) * 2;   // bytes of one complex
+    const size_t spin_bytes = (size_t)g.vh * 4 * nc * m * rb;
+    const size_t gauge_bytes = (size_t)8 * g.vh * nc * nc * rb;
+    void *in = nullptr, *out = nullptr, *gauge = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = QCU_SUCCESS;
+    auto cleanup = [&]() {
+        if (in) cudaFree(in);
+        if (out) cudaFree(out);
+        if (gauge) cudaFree(gauge);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    if (cudaMalloc(&in, spin_bytes) != cudaSuccess || cudaMalloc(&out, spin_bytes) != cudaSuccess ||
+        cudaMalloc(&gauge, gauge_bytes) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return -set_error(QCU_ERR_ALLOC, "autotuner: device allocation failed");
+    }
+    fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(in), (int64_t)(spin_bytes / 4), 1u);
+    fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(gauge), (int64_t)(gauge_bytes / 4), 2u);
+    const int saved = hop_kind();
+    int kinds[3] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR};
+    int best = QCU_HOP_SIMT;
+    float best_ms = 1e30f;
+    for (int kind : kinds) {
+        if (kind == QCU_HOP_SIMT_CS && nc * m > kRedThreads) continue;
+        if (kind == QCU_HOP_TENSOR && !hop_tc_supported(nc, m, prec)) continue;
+        set_hop_kind(kind);
+        HopParams p{};
+        p.in = in;
+        p.out = out;
+        p.gauge = gauge;
+        p.g = g;
+        p.m = m;
+        p.t_sign = 1.0;
+        for (int i = 0; i < 2 && rc == QCU_SUCCESS; ++i) {
+            p.parity = i & 1;
+            rc = hop_launch(p, nc, prec, false, EPI_PLAIN, st);
+        }
+        if (rc) break;
+        const int reps = 5;
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < reps && rc == QCU_SUCCESS; ++i) {
+            p.parity = i & 1;
+            rc = hop_launch(p, nc, prec, false, EPI_PLAIN, st);
+        }
+        cudaEventRecord(e1, st);
+        if (rc) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = set_error(QCU_ERR_CUDA, "autotuner: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= reps;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kind;
+        }
+    }
+    set_hop_kind(saved);
+    cleanup();
+    if (rc) return -rc;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        load_cache_locked();
+        g_tuned[std::make_tuple(current_device(), nc, m, prec)] = best;
+        const char* path = std::getenv("QCU_TUNE_CACHE");
+        if (path && *path) {
+            if (FILE* f = std::fopen(path, "a")) {
+                std::fprintf(f, "%d %d %d %d %.3f\n", nc, m, prec, best, best_ms * 1e3);
+                std::fclose(f);
+            }
+        }
+    }
+    if (best_us) *best_us = best_ms * 1e3;
+    return best;
+}
+
+}  // namespace qcub
+
+using namespace qcub;
+
+extern "C" int qcuTuneHop(const int L[4], int n_color, int m_rhs, int precision, void* stream) {
+    clear_error();
+    if (!L) return -set_error(QCU_ERR_INVALID, "null lattice");
+    if (L[0] < 2 || L[0] % 2 || L[1] < 1 || L[2] < 1 || L[3] < 1)
+        return -set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d", L[0], L[1], L[2], L[3]);
+    if (n_color < 2 || n_color > kMaxColor) return -set_error(QCU_ERR_UNSUPPORTED, "n_color=%d", n_color);
+    if (m_rhs < 1 || m_rhs > kMaxRhs) return -set_error(QCU_ERR_INVALID, "m_rhs=%d", m_rhs);
+    return tune_hop(L, n_color, m_rhs, precision, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+extern "C" int qcuGetTunedHop(int n_color, int m_rhs, int precision) {
+    return tuned_hop(n_color, m_rhs, precision);
+}

@@ -91,9 +91,10 @@ def hop_kernel(request):
     q.lib().qcuSetHopKernel(q.HOP_AUTO)
 
 
-@pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT, q.HOP_TENSOR], indirect=True, ids=["simt", "tcgen05"])
+@pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR], indirect=True,
+                         ids=["simt", "simt_cs", "tcgen05"])
 @pytest.mark.parametrize("prec", [q.SINGLE, q.HALF, q.BF16])
-@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (8, 16), (2, 32), (6, 5)])
+@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (2, 32), (3, 17), (8, 16), (6, 5)])
 def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
     L = (8, 4, 4, 4)
     gauge, inp = _problem(L, nc, m, 40 + nc)
@@ -134,6 +135,35 @@ def test_tensor_core_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel):
     ref = oracle_lib.schur(ir, gr, L, 0.11, -1.0)
     assert rel_err(from_dev(d_out), ref) <= 2 * TOL[prec]
     assert q.lib().qcuGetKernelError(1) == 0
+
+
+@pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT, q.HOP_SIMT_CS], indirect=True, ids=["simt", "simt_cs"])
+@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (6, 8), (8, 16), (8, 32), (5, 3)])
+def test_fp64_hop_kernels(oracle_lib, nc, m, hop_kernel):
+    """Both SIMT work splits in FP64, with dagger and the antiperiodic boundary."""
+    L = (4, 2, 4, 6)
+    gauge, inp = _problem(L, nc, m, 90 + nc)
+    for parity in (0, 1):
+        for dagger in (False, True):
+            ref = oracle_lib.hop(inp, gauge, L, parity, dagger, -1.0)
+            got = _hop_gpu(inp, gauge, L, parity, dagger, -1.0, q.DOUBLE)
+            assert rel_err(got, ref) <= TOL[q.DOUBLE]
+
+
+@pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT_CS], indirect=True, ids=["simt_cs"])
+def test_colour_split_epilogues(oracle_lib, hop_kernel):
+    test_xpay_and_schur_epilogues(oracle_lib)
+
+
+def test_autotuner_records_a_valid_choice(tmp_path, monkeypatch):
+    L = (8, 4, 4, 8)
+    for prec in (q.DOUBLE, q.BF16):
+        k = q.lib().qcuTuneHop(q.lattice(L), 3, 12, prec, None)
+        assert k in (q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR), q.last_error()
+        assert q.lib().qcuGetTunedHop(3, 12, prec) == k
+        if prec == q.DOUBLE:
+            assert k != q.HOP_TENSOR
+    assert q.lib().qcuTuneHop(q.lattice((7, 4, 4, 4)), 3, 12, q.DOUBLE, None) < 0
 
 
 def test_xpay_and_schur_epilogues(oracle_lib):
