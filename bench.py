@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark: time to solve the multi-RHS Wilson-Dirac system to an FP64 true residual
-of 1e-10, mixed-precision (BF16 storage, FP32 arithmetic, FP64 reliable updates) vs the
-plain FP64 BiCGStab on the same GPU and fields, plus the dslash roofline fraction.
+of 1e-10, mixed-precision (FP16 storage, FP32 arithmetic, FP64 reliable updates; the
+BF16-storage solve is timed beside it) vs the plain FP64 BiCGStab on the same GPU and
+fields, plus the dslash roofline fraction and the per-precision dslash error.
 
 Workload: 24^3 x 48 lattice, SU(3), N_rhs = 12, kappa = 0.124, smoothed links
 U = exp(i 0.3 H), unit complex Gaussian sources, antiperiodic in t.  One step = one
@@ -40,7 +41,11 @@ WORKLOAD = "24^3x48 SU(3) Wilson-Dirac, N_rhs=12, kappa=0.124, smoothed links ep
            "antiperiodic t, BiCGStab to FP64 true residual 1e-10"
 # Plain FP64 BiCGStab iterations this system needs (measured with this benchmark's
 # plain leg on a B200); the CPU reference leg multiplies its per-iteration time by it.
-PLAIN_ITERS = None
+PLAIN_ITERS = 44
+# reliable-update threshold of the mixed solves (a sweep over 0.1 .. 0.003 on this
+# system gave the shortest time at 0.003 for FP16, BF16 and FP32 sloppy storage)
+RELIABLE_DELTA = 0.003
+CHECK_INTERVAL = 16
 
 
 def peaks():
@@ -204,14 +209,24 @@ def main():
     lib.getDslash(0, 1.0 / (2 * KAPPA) - 4.0)
     q.check()
 
-    def set_opts(solver, sloppy=q.BF16):
+    def set_opts(solver, sloppy=q.HALF):
         o = q.default_options()
         o.solver = solver
         o.sloppy_precision = sloppy
         o.stop_true_residual = 1
         o.t_boundary = T_BOUNDARY
-        o.check_interval = 16
+        o.check_interval = CHECK_INTERVAL
+        o.reliable_delta = RELIABLE_DELTA
         q.check(lib.qcuSetSolverOptions(ctypes.byref(o)))
+
+    # hop kernel per (N, m, precision) picked by the autotuner before anything is timed
+    tuned = {}
+    for name, prec in (("f64", q.DOUBLE), ("f16", q.HALF), ("bf16", q.BF16)):
+        k = lib.qcuTuneHop(q.lattice(L), NC, M, prec, None)
+        if k < 0:
+            raise RuntimeError(f"autotuner: {q.last_error()}")
+        tuned[name] = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16"}.get(k, str(k))
+    torch.cuda.synchronize()
 
     def solve(srcs, outs, max_iter=MAX_ITER):
         for j in range(M):
@@ -234,8 +249,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- mixed precision (the product path) ----
-    set_opts(q.SOLVER_MIXED)
+    # ---- mixed precision (the product path: FP16 storage) ----
+    set_opts(q.SOLVER_MIXED, q.HALF)
     for _ in range(args.warmup):
         stats = solve(d_src, d_x)
     clocks = ClockSampler(torch.cuda.current_device())
@@ -254,6 +269,16 @@ def main():
     clk = clocks.stop()
     reliable = stats.reliable_updates
 
+    # ---- the same solve with BF16 storage ----
+    set_opts(q.SOLVER_MIXED, q.BF16)
+    solve(d_src, d_x)
+    barrier()
+    ev0.record()
+    stats_bf = solve(d_src, d_x)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_bf16 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+
     # ---- plain FP64 BiCGStab (same fields, same GPU) ----
     set_opts(q.SOLVER_FUSED)
     try:
@@ -269,17 +294,35 @@ def main():
     it_plain = stats_plain.iterations
     rel_plain = max(stats_plain.true_residual[:M])
 
-    # ---- dslash roofline: BF16 hop on the gathered layout (dominant kernel of the solve) ----
+    # ---- dslash roofline: the FP16 hop (dominant kernel of the solve), BF16 and FP64 beside it;
+    #      dslash error of each storage precision against the FP64 hop (which matches the
+    #      reference's kernels to 1e-13) on the benchmark's gauge field and a Gaussian spinor ----
     hbm, peak_kind = peaks()
     stream = torch.cuda.current_stream()
     dev_stream = ctypes.c_void_p(stream.cuda_stream)
     roof = {}
-    for name, prec, dt in (("bf16", q.BF16, torch.bfloat16), ("f64", q.DOUBLE, torch.float64)):
-        s = q.PREC_BYTES[prec]
+    Lc = q.lattice(L)
+    gen = torch.Generator(device="cpu").manual_seed(11)
+    psi64 = torch.randn((vh, 4, NC, M, 2), generator=gen, dtype=torch.float64).cuda()
+    ref_out = torch.empty_like(psi64)
+    q.check(lib.qcuDslashMrhs(ref_out.data_ptr(), psi64.data_ptr(), d_gauge.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
+                              q.DOUBLE, dev_stream))
+    dslash_err = {}
+    for name, prec, dt in (("f16", q.HALF, torch.float16), ("bf16", q.BF16, torch.bfloat16),
+                           ("f32", q.SINGLE, torch.float32), ("f64", q.DOUBLE, torch.float64)):
+        s_b = q.PREC_BYTES[prec]
         g_l = d_gauge.to(dt)
-        a = torch.randn((vh, 4, NC, M, 2), device="cuda").to(dt)
+        a = psi64.to(dt)
         out = torch.empty_like(a)
-        Lc = q.lattice(L)
+        q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
+                                  prec, dev_stream))
+        torch.cuda.synchronize()
+        if prec != q.DOUBLE:
+            dslash_err[name] = float(torch.linalg.vector_norm(out.double() - ref_out) /
+                                     torch.linalg.vector_norm(ref_out))
+        if name == "f32":
+            del g_l, a, out
+            continue
         for _ in range(3):
             q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
                                       prec, dev_stream))
@@ -293,12 +336,13 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         dur = e0.elapsed_time(e1) / 1e3 / reps
-        byts = hop_bytes(vh, NC, M, s)
+        byts = hop_bytes(vh, NC, M, s_b)
         roof[name] = {"bound": "hbm", "achieved": byts / dur / 1e9, "peak": hbm, "unit": "GB/s",
                       "frac": byts / dur / 1e9 / hbm, "traffic": None, "launch_us": dur * 1e6,
                       "algorithmic_bytes": byts, "gflops": hop_flops(vh, NC, M) / dur / 1e9,
-                      "peak_kind": f"{peak_kind} HBM copy bandwidth"}
+                      "kernel": tuned[name], "peak_kind": f"{peak_kind} HBM copy bandwidth"}
         del g_l, a, out
+    del psi64, ref_out
 
     # ---- end to end through the C ABI with host buffers ----
     h_gauge = torch.empty(d_gauge.shape, dtype=d_gauge.dtype, pin_memory=True)
@@ -307,7 +351,7 @@ def main():
     for j in range(M):
         h_src[j].copy_(d_src[j])
     h_x = [torch.empty_like(h_src[0]) for _ in range(M)]
-    set_opts(q.SOLVER_MIXED)
+    set_opts(q.SOLVER_MIXED, q.HALF)
     barrier()
     ev0.record()
     for _ in range(args.steps):
@@ -329,7 +373,7 @@ def main():
 
     # kernels launched per mixed solve: setup + 12 per graphed iteration (7 BiCGStab + 5 gated
     # reliable-update kernels) rounded up to the graph length + reconstruction/statistics
-    interval = 16
+    interval = CHECK_INTERVAL
     graphed = -(-it_mixed[-1] // interval) * interval
     launches_per_solve = 4 + 9 + 12 * graphed + 1 + 4 + 4
     gpu_launches = launches_per_solve * args.steps
@@ -343,17 +387,24 @@ def main():
         line = {
             "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
-            "dtype_detail": "BF16 storage, FP32 arithmetic, FP64 reductions and reliable updates",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+            "dtype_detail": "FP16 storage, FP32 arithmetic, FP64 reductions, reliable updates and solution",
             "data": "synthetic: seeded smoothed SU(3) links exp(i 0.3 H), unit complex Gaussian sources",
             "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA,
                        "tol": TOL, "l2": "inputs larger than L2 (each hop reads 478 MB in BF16, 1.9 GB in FP64)",
-                       "replicas": world},
+                       "replicas": world, "reliable_delta": RELIABLE_DELTA, "check_interval": CHECK_INTERVAL,
+                       "hop_kernels": tuned},
             "solves_per_s_all_ranks": world / t_mixed,
             "mixed": {"iterations": it_mixed[-1], "reliable_updates": reliable, "true_residual_max": max(rel_mixed)},
+            "mixed_bf16": {"value": t_bf16, "unit": "s", "iterations": stats_bf.iterations,
+                           "reliable_updates": stats_bf.reliable_updates,
+                           "true_residual_max": max(stats_bf.true_residual[:M]),
+                           "speedup_vs_plain": t_plain / t_bf16},
+            "dslash_rel_err_vs_fp64": dslash_err,
             "plain_fp64": {"value": t_plain, "unit": "s", "iterations": it_plain, "true_residual_max": rel_plain,
                            "speedup_mixed_vs_plain": t_plain / t_mixed},
-            "roofline": roof["bf16"],
+            "roofline": roof["f16"],
+            "roofline_bf16_hop": roof["bf16"],
             "roofline_fp64_hop": roof["f64"],
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "clocks": clk,

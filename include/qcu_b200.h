@@ -48,6 +48,9 @@ const char *qcuGetLastError(void);
 #define QCU_SOLVER_REFERENCE 0 /* reference policy-1 BiCGStab, output precision, recursive residual */
 #define QCU_SOLVER_FUSED 1     /* same iteration, fused device-resident kernels, CUDA graph */
 #define QCU_SOLVER_MIXED 2     /* sloppy-precision inner BiCGStab with FP64 reliable updates */
+#define QCU_SOLVER_PRECOND 3   /* FP64 BiCGStab on the full system, right-preconditioned by the
+                                  learned preconditioner of qcuSetPreconditioner; falls back to
+                                  QCU_SOLVER_FUSED if it does not converge */
 
 typedef struct {
     int solver;              /* QCU_SOLVER_* (default QCU_SOLVER_FUSED) */
@@ -75,10 +78,82 @@ typedef struct {
     double true_residual[QCU_MAX_RHS];      /* ||b - M x|| / ||b|| per RHS, full system, FP64 */
     double recursive_residual[QCU_MAX_RHS]; /* last recursive Schur residual ||r|| / ||b'|| */
     double solve_seconds;    /* device time of the solve (gather..scatter), CUDA events */
+    int fallback;            /* PRECOND: 1 when the plain solver had to finish the solve */
+    int precond_iterations;  /* PRECOND: iterations of the preconditioned BiCGStab */
 } QcuSolveStats;
 
 /* Statistics of the last qcuInvert on the current context. */
 int qcuGetSolveStats(QcuSolveStats *stats);
+
+/* ---- batched solves of independent systems ----
+ * No counterpart in the reference (its Qcu object holds one system).  Each system has
+ * its own lattice, colour count, RHS count, kappa, tolerance and gauge field; all are
+ * solved together on the current GPU with the even/odd Schur BiCGStab selected by
+ * `opts` (NULL: defaults), one CUDA graph holding every system as an independent
+ * branch.  Fields are FP64 device pointers in the qcu.h layouts: gauge EO
+ * [4][2][Vh][N][N], each b[j] / x[j] a full-lattice EO fermion [2][Vh][4][N].
+ * Outputs are written into the struct.  Returns QCU_SUCCESS when every system
+ * converged, else the first failing status (every x is still written). */
+typedef struct {
+    int lattice_size[4];    /* X, Y, Z, T */
+    int n_color;
+    int m_rhs;
+    double kappa;
+    double tol;             /* per-RHS relative tolerance, as in qcuInvert */
+    int max_iteration;
+    const void *gauge;
+    void *const *b;         /* m_rhs source pointers */
+    void *const *x;         /* m_rhs solution pointers */
+    /* outputs */
+    int iterations;
+    int reliable_updates;
+    int status;
+    double true_residual_max;  /* max_j ||b_j - M x_j|| / ||b_j|| (FP64) */
+    double latency_seconds;    /* from the start of the iterations to this system's convergence */
+} QcuBatchSystem;
+
+/* ---- learned gauge-covariant preconditioner ----
+ * No counterpart in the reference.  P is a stack of `layers` parallel-transport
+ * convolutions with channels 1 -> C -> ... -> C -> 1 and no nonlinearity, so it is a
+ * fixed linear operator that commutes with gauge transformations:
+ *   out_o(x) = sum_i sum_k W[o][i][k] (T_k in_i)(x),  k = 0..8,
+ *   T_0 = 1,  T_{1+2mu} f(x) = U_mu(x) f(x+mu),  T_{2+2mu} f(x) = U_mu(x-mu)^dag f(x-mu)
+ * (hops across the t boundary carry t_boundary), W[o][i][k] a complex 4x4 spin matrix.
+ * Weights are FP32 complex (re, im interleaved), layer-major [layer][cout][cin][9][4][4].
+ * Fields are gathered full-lattice multi-RHS spinors [2][Vh][4][N][m] (even half first)
+ * on the device, FP32 or FP64.  Training minimises sum_j ||M P b_j - b_j||^2 / ||b_j||^2
+ * (M = 1 - kappa D) with the library's own forward, adjoint and weight-gradient kernels
+ * and Adam.  2 <= n_color <= 4. */
+int qcuPrecondCreate(void **handle, const int L[4], int n_color, int m_rhs, int layers, int channels,
+                     double t_boundary);
+int qcuPrecondDestroy(void *handle);
+/* number of complex weights (negative status on error) */
+int64_t qcuPrecondNumWeights(void *handle);
+/* host arrays of 2 * qcuPrecondNumWeights floats; setting the weights resets Adam */
+int qcuPrecondSetWeights(void *handle, const float *weights);
+int qcuPrecondGetWeights(void *handle, float *weights);
+/* EO gauge field [4][2][Vh][N][N] on the device, kept as an FP32 copy */
+int qcuPrecondSetGauge(void *handle, const void *gauge, int precision);
+/* out = P in on `stream` */
+int qcuPrecondApply(void *handle, void *out, const void *in, int precision, void *stream);
+/* loss and, if grad is not NULL, d loss / d(Re w, Im w) as 2 * NumWeights doubles */
+int qcuPrecondLossGrad(void *handle, const void *b, int precision, double kappa, double *loss, double *grad);
+/* one Adam step (beta 0.9, 0.999) on the loss of the m right-hand sides b */
+int qcuPrecondTrainStep(void *handle, const void *b, int precision, double kappa, double lr, double *loss);
+/* attach P to the qcu.h context for QCU_SOLVER_PRECOND (NULL detaches); its lattice,
+ * n_color and m_rhs must match the context's */
+int qcuSetPreconditioner(void *handle);
+
+/* flags of qcuInvertBatch */
+#define QCU_BATCH_DEVICE_LOOP 0 /* one graph launch; each system loops in a conditional graph node */
+#define QCU_BATCH_HOST_LOOP 1   /* the host relaunches the graph every check_interval iterations */
+#define QCU_BATCH_KEEP_CONTEXTS 2 /* keep each system's context and device buffers after the call;
+                                     a later batch reuses them for systems of the same lattice,
+                                     n_color and m_rhs (qcuBatchRelease frees them) */
+
+int qcuInvertBatch(QcuBatchSystem *systems, int n_systems, const QcuSolverOptions *opts, int flags);
+/* free the contexts kept by QCU_BATCH_KEEP_CONTEXTS */
+int qcuBatchRelease(void);
 
 /* ---- device-level entry points (caller-owned device buffers) ----
  * Gathered multi-RHS layout, one parity: [Vh][4][Nc][m] complex.
@@ -160,12 +235,20 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
  *   TENSOR   FP16/BF16 storage on the tcgen05 tensor cores with TMEM accumulators and
  *            bulk-copy (TMA) staged neighbour spinors, for 2 <= n_color <= 4 and
  *            m_rhs <= 32 (else SIMT);
+ *   PACKED16 FP16/BF16 storage, links staged once per site in shared memory, projection
+ *            and link products in packed 16-bit complex arithmetic, the 8 hops summed
+ *            in FP32; 2 <= n_color <= 4, m_rhs >= 2 (else SIMT);
+ *   PACKED16_ACC16  as PACKED16, with the 8 hops also summed in FP16 (FP16 storage
+ *            only; the accumulation of the reference's half-precision path); less
+ *            accurate, so AUTO never picks it;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else a static rule. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2
 #define QCU_HOP_SIMT_CS 3
+#define QCU_HOP_PACKED16 4
+#define QCU_HOP_PACKED16_ACC16 5
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

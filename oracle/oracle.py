@@ -52,6 +52,9 @@ def lib():
         for name in ("oracle_gauge_to_eo", "oracle_gauge_from_eo", "oracle_fermion_to_eo",
                      "oracle_fermion_from_eo"):
             getattr(l, name).argtypes = [_dp, _dp, _ip, ctypes.c_int]
+        for name in ("oracle_ptc_forward", "oracle_ptc_adjoint", "oracle_ptc_wgrad"):
+            getattr(l, name).argtypes = [_dp, _dp, _dp, _dp, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_double]
         l.oracle_set_threads.argtypes = [ctypes.c_int]
         l.oracle_get_threads.restype = ctypes.c_int
         _lib = l
@@ -199,3 +202,75 @@ def fermion_from_eo(eo, L):
     lex = np.empty_like(eo)
     lib().oracle_fermion_from_eo(_ptr(lex), _ptr(eo), _L(L), nc)
     return lex
+
+
+# ---------------- learned preconditioner (parallel-transport convolution net) ----------------
+
+def ptc_forward(inp, w, gauge, L, t_sign=1.0):
+    """One layer: inp [cin][2][Vh][4][N][m], w [cout][cin][9][4][4] -> [cout][2][Vh][4][N][m]."""
+    inp = _c(inp); w = _c(w); gauge = _c(gauge)
+    cin, nc, m = inp.shape[0], inp.shape[4], inp.shape[5]
+    cout = w.shape[0]
+    assert w.shape[1] == cin
+    out = np.empty((cout,) + inp.shape[1:], dtype=np.complex128)
+    lib().oracle_ptc_forward(_ptr(out), _ptr(inp), _ptr(w), _ptr(gauge), _L(L), nc, m, cin, cout, float(t_sign))
+    return out
+
+
+def ptc_adjoint(gout, w, gauge, L, t_sign=1.0):
+    """Adjoint of one layer: gout [cout][...] -> gin [cin][...]."""
+    gout = _c(gout); w = _c(w); gauge = _c(gauge)
+    cout, cin = w.shape[0], w.shape[1]
+    nc, m = gout.shape[4], gout.shape[5]
+    gin = np.empty((cin,) + gout.shape[1:], dtype=np.complex128)
+    lib().oracle_ptc_adjoint(_ptr(gin), _ptr(gout), _ptr(w), _ptr(gauge), _L(L), nc, m, cin, cout, float(t_sign))
+    return gin
+
+
+def ptc_wgrad(gout, inp, gauge, L, t_sign=1.0):
+    """Complex weight gradient tensor gw[cout][cin][9][4][4] of one layer."""
+    gout = _c(gout); inp = _c(inp); gauge = _c(gauge)
+    cout, cin = gout.shape[0], inp.shape[0]
+    nc, m = inp.shape[4], inp.shape[5]
+    gw = np.empty((cout, cin, 9, 4, 4), dtype=np.complex128)
+    lib().oracle_ptc_wgrad(_ptr(gw), _ptr(gout), _ptr(inp), _ptr(gauge), _L(L), nc, m, cin, cout, float(t_sign))
+    return gw
+
+
+def _full_to_per_rhs(v):
+    """gathered full lattice [2][Vh][4][N][m] -> per-RHS [m][2][Vh][4][N]"""
+    return np.ascontiguousarray(np.moveaxis(v, -1, 0))
+
+
+def _per_rhs_to_full(v):
+    return np.ascontiguousarray(np.moveaxis(v, 0, -1))
+
+
+def precond_apply(b, weights, gauge, L, t_sign=1.0):
+    """P b for the layer stack `weights` (list of [cout][cin][9][4][4]); b [2][Vh][4][N][m]."""
+    a = _c(b)[None]
+    for w in weights:
+        a = ptc_forward(a, w, gauge, L, t_sign)
+    return a[0]
+
+
+def precond_loss_grad(b, weights, gauge, L, kappa, t_sign=1.0):
+    """Loss sum_j ||M P b_j - b_j||^2 / ||b_j||^2 and its gradient with respect to the real
+    and imaginary parts of every weight (list of complex arrays: grad = dL/dRe + i dL/dIm)."""
+    b = _c(b)
+    acts = [b[None]]
+    for w in weights:
+        acts.append(ptc_forward(acts[-1], w, gauge, L, t_sign))
+    y = acts[-1][0]
+    r = _per_rhs_to_full(mat(_full_to_per_rhs(y), gauge, L, kappa, False, t_sign)) - b
+    bn2 = np.sum(np.abs(b) ** 2, axis=(0, 1, 2, 3))
+    loss = float(np.sum(np.sum(np.abs(r) ** 2, axis=(0, 1, 2, 3)) / bn2))
+    g = _per_rhs_to_full(mat(_full_to_per_rhs(r), gauge, L, kappa, True, t_sign)) / bn2
+    g = g[None]
+    grads = [None] * len(weights)
+    for li in range(len(weights) - 1, -1, -1):
+        gw = ptc_wgrad(g, acts[li], gauge, L, t_sign)
+        grads[li] = 2.0 * gw
+        if li > 0:
+            g = ptc_adjoint(g, weights[li], gauge, L, t_sign)
+    return loss, grads

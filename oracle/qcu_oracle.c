@@ -394,3 +394,140 @@ void oracle_fermion_to_eo(double* eo, const double* lex, const int L[4], int nc)
 void oracle_fermion_from_eo(double* lex, const double* eo, const int L[4], int nc) {
     reorder_sites(lex, eo, L, 4L * nc, 0);
 }
+
+/* ---------------- parallel-transport convolution (learned preconditioner layer) ----------------
+ * Path k: 0 identity, 1 + 2 mu: U_mu(x) f(x + mu), 2 + 2 mu: U_mu(x - mu)^dag f(x - mu).
+ * Fields are gathered full-lattice multi-RHS spinors [ch][2][Vh][4][nc][m]. */
+
+static int ptc_opposite(int k) { return k == 0 ? 0 : (((k - 1) & 1) ? k - 1 : k + 1); }
+
+/* (T_k f)(x) for every spin, colour and RHS of site x = (parity, idx) of one channel */
+static void ptc_transport(cplx* res, const cplx* f, const cplx* gauge, const int L[4], int nc, int m,
+                          int parity, long idx, int k, double t_sign) {
+    const long vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+    const long site_len = 4L * nc * m;
+    if (k == 0) {
+        memcpy(res, f + ((long)parity * vh + idx) * site_len, sizeof(cplx) * site_len);
+        return;
+    }
+    const int mu = (k - 1) >> 1, fwd = ((k - 1) & 1) == 0;
+    int xh, y, z, t;
+    half_coords(idx, L, &xh, &y, &z, &t);
+    const int x = 2 * xh + ((parity + y + z + t) & 1);
+    int wrap;
+    const long nb = neighbour(x, y, z, t, mu, fwd ? +1 : -1, L, &wrap);
+    const cplx* link = fwd ? gauge + (((long)mu * 2 + parity) * vh + idx) * nc * nc
+                           : gauge + (((long)mu * 2 + (1 - parity)) * vh + nb) * nc * nc;
+    const cplx* src = f + ((long)(1 - parity) * vh + nb) * site_len;
+    const double sg = wrap ? t_sign : 1.0;
+    for (int s = 0; s < 4; ++s)
+        for (int c = 0; c < nc; ++c)
+            for (int r = 0; r < m; ++r) {
+                cplx acc = 0;
+                for (int cc = 0; cc < nc; ++cc) {
+                    const cplx u = fwd ? link[c * nc + cc] : conj(link[cc * nc + c]);
+                    acc += u * src[((long)s * nc + cc) * m + r];
+                }
+                res[((long)s * nc + c) * m + r] = sg * acc;
+            }
+}
+
+void oracle_ptc_forward(double* out_d, const double* in_d, const double* w_d, const double* gauge_d,
+                        const int L[4], int nc, int m, int cin, int cout, double t_sign) {
+    const long vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+    const long site_len = 4L * nc * m, field = 2 * vh * site_len;
+    const cplx* in = (const cplx*)in_d;
+    const cplx* w = (const cplx*)w_d;
+    const cplx* gauge = (const cplx*)gauge_d;
+    cplx* out = (cplx*)out_d;
+#pragma omp parallel
+    {
+        cplx* tr = (cplx*)malloc(sizeof(cplx) * site_len);
+#pragma omp for schedule(static)
+        for (long site = 0; site < 2 * vh; ++site) {
+            const int parity = (int)(site / vh);
+            const long idx = site % vh;
+            for (int o = 0; o < cout; ++o) memset(out + o * field + site * site_len, 0, sizeof(cplx) * site_len);
+            for (int i = 0; i < cin; ++i)
+                for (int k = 0; k < 9; ++k) {
+                    ptc_transport(tr, in + i * field, gauge, L, nc, m, parity, idx, k, t_sign);
+                    for (int o = 0; o < cout; ++o) {
+                        const cplx* W = w + (((long)o * cin + i) * 9 + k) * 16;
+                        cplx* dst = out + o * field + site * site_len;
+                        for (int sp = 0; sp < 4; ++sp)
+                            for (int s = 0; s < 4; ++s) {
+                                const cplx ws = W[sp * 4 + s];
+                                if (ws == 0) continue;
+                                for (long e = 0; e < (long)nc * m; ++e) dst[sp * nc * m + e] += ws * tr[s * nc * m + e];
+                            }
+                    }
+                }
+        }
+        free(tr);
+    }
+}
+
+void oracle_ptc_adjoint(double* gin_d, const double* gout_d, const double* w_d, const double* gauge_d,
+                        const int L[4], int nc, int m, int cin, int cout, double t_sign) {
+    const long vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+    const long site_len = 4L * nc * m, field = 2 * vh * site_len;
+    const cplx* gout = (const cplx*)gout_d;
+    const cplx* w = (const cplx*)w_d;
+    const cplx* gauge = (const cplx*)gauge_d;
+    cplx* gin = (cplx*)gin_d;
+#pragma omp parallel
+    {
+        cplx* tr = (cplx*)malloc(sizeof(cplx) * site_len);
+#pragma omp for schedule(static)
+        for (long site = 0; site < 2 * vh; ++site) {
+            const int parity = (int)(site / vh);
+            const long idx = site % vh;
+            for (int i = 0; i < cin; ++i) memset(gin + i * field + site * site_len, 0, sizeof(cplx) * site_len);
+            for (int o = 0; o < cout; ++o)
+                for (int k = 0; k < 9; ++k) {
+                    /* T_k^dag = T_opposite(k); the spin matrix enters conjugate-transposed */
+                    ptc_transport(tr, gout + o * field, gauge, L, nc, m, parity, idx, ptc_opposite(k), t_sign);
+                    for (int i = 0; i < cin; ++i) {
+                        const cplx* W = w + (((long)o * cin + i) * 9 + k) * 16;
+                        cplx* dst = gin + i * field + site * site_len;
+                        for (int s = 0; s < 4; ++s)
+                            for (int sp = 0; sp < 4; ++sp) {
+                                const cplx ws = conj(W[sp * 4 + s]);
+                                if (ws == 0) continue;
+                                for (long e = 0; e < (long)nc * m; ++e) dst[s * nc * m + e] += ws * tr[sp * nc * m + e];
+                            }
+                    }
+                }
+        }
+        free(tr);
+    }
+}
+
+void oracle_ptc_wgrad(double* gw_d, const double* gout_d, const double* in_d, const double* gauge_d,
+                      const int L[4], int nc, int m, int cin, int cout, double t_sign) {
+    const long vh = (long)L[0] * L[1] * L[2] * L[3] / 2;
+    const long site_len = 4L * nc * m, field = 2 * vh * site_len;
+    const cplx* gout = (const cplx*)gout_d;
+    const cplx* in = (const cplx*)in_d;
+    const cplx* gauge = (const cplx*)gauge_d;
+    cplx* gw = (cplx*)gw_d;
+    const long nw = (long)cout * cin * 9;
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < nw; ++q) {
+        const int k = (int)(q % 9), i = (int)((q / 9) % cin), o = (int)(q / (9L * cin));
+        cplx acc[16] = {0};
+        cplx* tr = (cplx*)malloc(sizeof(cplx) * site_len);
+        for (long site = 0; site < 2 * vh; ++site) {
+            ptc_transport(tr, in + i * field, gauge, L, nc, m, (int)(site / vh), site % vh, k, t_sign);
+            const cplx* g = gout + o * field + site * site_len;
+            for (int sp = 0; sp < 4; ++sp)
+                for (int s = 0; s < 4; ++s) {
+                    cplx a = 0;
+                    for (long e = 0; e < (long)nc * m; ++e) a += g[sp * nc * m + e] * conj(tr[s * nc * m + e]);
+                    acc[sp * 4 + s] += a;
+                }
+        }
+        free(tr);
+        for (int e = 0; e < 16; ++e) gw[q * 16 + e] = acc[e];
+    }
+}

@@ -81,6 +81,24 @@ void oracle_gauge_from_eo(double* lex, const double* eo, const int L[4], int nc)
 void oracle_fermion_to_eo(double* eo, const double* lex, const int L[4], int nc);
 void oracle_fermion_from_eo(double* lex, const double* eo, const int L[4], int nc);
 
+/* Gauge-covariant parallel-transport convolution, the layer of the learned
+ * preconditioner (no reference code; restated from its definition).
+ * Fields: `ch` channels of gathered full-lattice multi-RHS spinors [ch][2][Vh][4][Nc][m].
+ * Weights w[cout][cin][9][4][4] complex, one 4x4 spin matrix per (out, in, path).
+ * Path k: 0 identity; 1 + 2 mu: U_mu(x) f(x + mu); 2 + 2 mu: U_mu(x - mu)^dag f(x - mu);
+ * a hop that wraps in t is multiplied by t_sign.
+ *   forward:  out_o(x) = sum_i sum_k w[o][i][k] (T_k in_i)(x)
+ *   adjoint:  gin_i    = sum_o sum_k w[o][i][k]^dag T_k^dag gout_o   (T_k^dag = T_{-k})
+ *   wgrad:    gw[o][i][k][s'][s] = sum_{x,c,r} gout_o(x)[s'][c][r] conj((T_k in_i)(x)[s][c][r])
+ * For a real loss with gout = dLoss/d(out*), the gradient with respect to the real and
+ * imaginary parts of w is 2 Re(gw), 2 Im(gw). */
+void oracle_ptc_forward(double* out, const double* in, const double* w, const double* gauge,
+                        const int L[4], int nc, int m, int cin, int cout, double t_sign);
+void oracle_ptc_adjoint(double* gin, const double* gout, const double* w, const double* gauge,
+                        const int L[4], int nc, int m, int cin, int cout, double t_sign);
+void oracle_ptc_wgrad(double* gw, const double* gout, const double* in, const double* gauge,
+                      const int L[4], int nc, int m, int cin, int cout, double t_sign);
+
 /* Threads used by the OpenMP loops (0 = runtime default). */
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

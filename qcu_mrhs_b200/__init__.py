@@ -22,8 +22,8 @@ PREC_BYTES = {HALF: 2, SINGLE: 4, DOUBLE: 8, BF16: 2}
 # status codes
 SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_UNSUPPORTED, ERR_ALLOC = range(8)
 
-SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED = 0, 1, 2
-HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS = 0, 1, 2, 3
+SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND = 0, 1, 2, 3
+HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16 = 0, 1, 2, 3, 4, 5
 MAX_RHS = 64
 
 
@@ -57,8 +57,31 @@ class QcuSolveStats(ctypes.Structure):
         ("true_residual", ctypes.c_double * MAX_RHS),
         ("recursive_residual", ctypes.c_double * MAX_RHS),
         ("solve_seconds", ctypes.c_double),
+        ("fallback", ctypes.c_int),
+        ("precond_iterations", ctypes.c_int),
     ]
 
+
+class QcuBatchSystem(ctypes.Structure):
+    _fields_ = [
+        ("lattice_size", ctypes.c_int * 4),
+        ("n_color", ctypes.c_int),
+        ("m_rhs", ctypes.c_int),
+        ("kappa", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("max_iteration", ctypes.c_int),
+        ("gauge", ctypes.c_void_p),
+        ("b", ctypes.POINTER(ctypes.c_void_p)),
+        ("x", ctypes.POINTER(ctypes.c_void_p)),
+        ("iterations", ctypes.c_int),
+        ("reliable_updates", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("true_residual_max", ctypes.c_double),
+        ("latency_seconds", ctypes.c_double),
+    ]
+
+
+BATCH_DEVICE_LOOP, BATCH_HOST_LOOP, BATCH_KEEP_CONTEXTS = 0, 1, 2
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -85,6 +108,8 @@ _SIGNATURES = {
     "qcuGetDefaultSolverOptions": (None, [ctypes.POINTER(QcuSolverOptions)]),
     "qcuSetSolverOptions": (_i, [ctypes.POINTER(QcuSolverOptions)]),
     "qcuGetSolveStats": (_i, [ctypes.POINTER(QcuSolveStats)]),
+    "qcuInvertBatch": (_i, [ctypes.POINTER(QcuBatchSystem), _i, ctypes.POINTER(QcuSolverOptions), _i]),
+    "qcuBatchRelease": (_i, []),
     "qcuDslashMrhs": (_i, [_vp, _vp, _vp, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuDslashMrhsXpay": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuSchurMrhs": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _d, _i, _vp]),
@@ -109,6 +134,16 @@ _SIGNATURES = {
     "qcuTuneHop": (_i, [_ip, _i, _i, _i, _vp]),
     "qcuGetTunedHop": (_i, [_i, _i, _i]),
     "qcuDeviceSynchronize": (_i, []),
+    "qcuPrecondCreate": (_i, [ctypes.POINTER(_vp), _ip, _i, _i, _i, _i, _d]),
+    "qcuPrecondDestroy": (_i, [_vp]),
+    "qcuPrecondNumWeights": (_i64, [_vp]),
+    "qcuPrecondSetWeights": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "qcuPrecondGetWeights": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "qcuPrecondSetGauge": (_i, [_vp, _vp, _i]),
+    "qcuPrecondApply": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "qcuPrecondLossGrad": (_i, [_vp, _vp, _i, _d, ctypes.POINTER(_d), ctypes.POINTER(_d)]),
+    "qcuPrecondTrainStep": (_i, [_vp, _vp, _i, _d, _d, ctypes.POINTER(_d)]),
+    "qcuSetPreconditioner": (_i, [_vp]),
 }
 
 _lib = None

@@ -10,6 +10,7 @@
 #include "context.h"
 #include "dslash.h"
 #include "layout.h"
+#include "precond.h"
 
 namespace qcub {
 
@@ -68,7 +69,7 @@ static void default_options(QcuSolverOptions* o) {
     o->max_restarts = 0;
 }
 
-static void destroy_context(Context* c) {
+void context_destroy(Context* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     scratch_free(&c->ws);
@@ -78,6 +79,50 @@ static void destroy_context(Context* c) {
     if (c->ev_in) cudaEventDestroy(c->ev_in);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;   // DevBuf destructors free the buffers
+}
+
+// Validate the parameters and create the stream, events, scratch and scalars of a new
+// context (c is freshly constructed; on failure the caller destroys it).
+int context_init(Context* c, const int L[4], int n_color, int m_rhs, int in_prec, int dslash_prec) {
+    if (L[0] < 2 || L[0] % 2 || L[1] < 1 || L[2] < 1 || L[3] < 1)
+        return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", L[0], L[1], L[2], L[3]);
+    if (n_color < 2 || n_color > kMaxColor)
+        return set_error(QCU_ERR_UNSUPPORTED, "n_color=%d (supported 2..%d)", n_color, kMaxColor);
+    if (m_rhs < 1 || m_rhs > kMaxRhs) return set_error(QCU_ERR_INVALID, "m_rhs=%d (1..%d)", m_rhs, kMaxRhs);
+    if (!prec_valid(in_prec)) return set_error(QCU_ERR_INVALID, "input precision %d", in_prec);
+    if (!prec_valid(dslash_prec)) return set_error(QCU_ERR_INVALID, "dslash precision %d", dslash_prec);
+    c->g = make_geom(L);
+    c->nc = n_color;
+    c->m = m_rhs;
+    c->in_prec = in_prec;
+    c->dslash_prec = dslash_prec;
+    default_options(&c->opts);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(QCU_ERR_CUDA, "stream/event creation failed");
+    }
+    int rc = scratch_alloc(&c->ws);
+    if (!rc) rc = c->scalars.ensure(sizeof(BicgScalars));
+    if (!rc && cudaMallocHost(&c->host_sc, sizeof(BicgScalars)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = set_error(QCU_ERR_ALLOC, "pinned host allocation failed");
+    }
+    return rc;
+}
+
+int context_load_gauge(Context* c, const void* gauge, int prec) {
+    if (!gauge) return set_error(QCU_ERR_INVALID, "null gauge pointer");
+    if (!prec_valid(prec)) return set_error(QCU_ERR_INVALID, "gauge precision %d", prec);
+    const int D = QCU_PRECISION_DOUBLE;
+    int rc;
+    if ((rc = c->gauge[D].ensure((size_t)c->gauge_len() * 16))) return rc;
+    if ((rc = cast_complex(c->gauge[D].ptr, D, gauge, prec, c->gauge_len(), c->stream))) return rc;
+    for (int i = 0; i < 5; ++i) c->gauge_valid[i] = false;
+    c->gauge_valid[D] = true;
+    c->gauge_loaded = true;
+    return QCU_SUCCESS;
 }
 
 static int require_ctx() {
@@ -113,38 +158,13 @@ static int init_impl(QcuGrid* grid, QcuParam* param, int n_color, int m_rhs, int
         if (grid->grid_size[i] != 1)
             return set_error(QCU_ERR_UNSUPPORTED, "process grid %d,%d,%d,%d: one GPU needs 1,1,1,1",
                              grid->grid_size[0], grid->grid_size[1], grid->grid_size[2], grid->grid_size[3]);
-    const int* L = param->lattice_size;
-    if (L[0] < 2 || L[0] % 2 || L[1] < 1 || L[2] < 1 || L[3] < 1)
-        return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", L[0], L[1], L[2], L[3]);
-    if (n_color < 2 || n_color > kMaxColor)
-        return set_error(QCU_ERR_UNSUPPORTED, "n_color=%d (supported 2..%d)", n_color, kMaxColor);
-    if (m_rhs < 1 || m_rhs > kMaxRhs) return set_error(QCU_ERR_INVALID, "m_rhs=%d (1..%d)", m_rhs, kMaxRhs);
-    if (!prec_valid(in_prec)) return set_error(QCU_ERR_INVALID, "input precision %d", in_prec);
-    if (!prec_valid(dslash_prec)) return set_error(QCU_ERR_INVALID, "dslash precision %d", dslash_prec);
-    if (g_ctx) {
-        destroy_context(g_ctx);
-        g_ctx = nullptr;
-    }
     Context* c = new Context();
-    c->g = make_geom(L);
-    c->nc = n_color;
-    c->m = m_rhs;
-    c->in_prec = in_prec;
-    c->dslash_prec = dslash_prec;
-    default_options(&c->opts);
-    int rc = QCU_SUCCESS;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess)
-        rc = set_error(QCU_ERR_CUDA, "stream/event creation failed");
-    if (!rc) rc = scratch_alloc(&c->ws);
-    if (!rc) rc = c->scalars.ensure(sizeof(BicgScalars));
-    if (!rc && cudaMallocHost(&c->host_sc, sizeof(BicgScalars)) != cudaSuccess)
-        rc = set_error(QCU_ERR_ALLOC, "pinned host allocation failed");
+    const int rc = context_init(c, param->lattice_size, n_color, m_rhs, in_prec, dslash_prec);
     if (rc) {
-        destroy_context(c);
+        context_destroy(c);
         return rc;
     }
+    context_destroy(g_ctx);
     g_ctx = c;
     return QCU_SUCCESS;
 }
@@ -154,14 +174,8 @@ static int load_gauge_impl(void* gauge, int prec) {
     if (rc) return rc;
     Context& c = *g_ctx;
     if (!gauge) return set_error(QCU_ERR_INVALID, "null gauge pointer");
-    if (!prec_valid(prec)) return set_error(QCU_ERR_INVALID, "gauge precision %d", prec);
-    const int D = QCU_PRECISION_DOUBLE;
     if ((rc = order_after_caller(c))) return rc;
-    if ((rc = c.gauge[D].ensure((size_t)c.gauge_len() * 16))) return rc;
-    if ((rc = cast_complex(c.gauge[D].ptr, D, gauge, prec, c.gauge_len(), c.stream))) return rc;
-    for (int i = 0; i < 5; ++i) c.gauge_valid[i] = false;
-    c.gauge_valid[D] = true;
-    c.gauge_loaded = true;
+    if ((rc = context_load_gauge(&c, gauge, prec))) return rc;
     QCUB_CUDA_CHECK(cudaStreamSynchronize(c.stream));
     return QCU_SUCCESS;
 }
@@ -292,7 +306,10 @@ static int invert_impl(int max_iter, double tol) {
     for (int par = 0; par < 2; ++par)
         if ((rc = gather_mrhs(b + par * hb, P, ins[par], P, c.g.vh, c.nc, c.m, c.stream))) return rc;
     c.stats = QcuSolveStats{};
-    rc = mixed ? solve_mixed(c, x, b, max_iter, tol) : solve_fused(c, x, b, max_iter, tol);
+    if (c.opts.solver == QCU_SOLVER_PRECOND)
+        rc = solve_precond(c, c.precond, x, b, max_iter, tol);
+    else
+        rc = mixed ? solve_mixed(c, x, b, max_iter, tol) : solve_fused(c, x, b, max_iter, tol);
     const int solve_rc = rc;
     if (rc != QCU_SUCCESS && rc != QCU_ERR_NOT_CONVERGED && rc != QCU_ERR_BREAKDOWN) return rc;
     // write the solution (also the last iterate when not converged)
@@ -365,7 +382,7 @@ void qcuInvert(int max_iteration, double p_max_prec) {
 
 void finalizeQcu() {
     QCUB_API_BEGIN
-    destroy_context(g_ctx);
+    context_destroy(g_ctx);
     g_ctx = nullptr;
 }
 
@@ -401,11 +418,26 @@ int qcuSetSolverOptions(const QcuSolverOptions* opts) {
     int rc = require_ctx();
     if (rc) return rc;
     if (!opts) return set_error(QCU_ERR_INVALID, "null options");
-    if (opts->solver < QCU_SOLVER_REFERENCE || opts->solver > QCU_SOLVER_MIXED)
+    if (opts->solver < QCU_SOLVER_REFERENCE || opts->solver > QCU_SOLVER_PRECOND)
         return set_error(QCU_ERR_INVALID, "solver %d", opts->solver);
     if (opts->t_boundary != 1.0 && opts->t_boundary != -1.0)
         return set_error(QCU_ERR_INVALID, "t_boundary must be +1 or -1");
     g_ctx->opts = *opts;
+    return QCU_SUCCESS;
+}
+
+int qcuSetPreconditioner(void* handle) {
+    QCUB_API_BEGIN
+    int rc = require_ctx();
+    if (rc) return rc;
+    Precond* P = static_cast<Precond*>(handle);
+    if (P) {
+        for (int i = 0; i < 4; ++i)
+            if (P->g.L[i] != g_ctx->g.L[i]) return set_error(QCU_ERR_INVALID, "preconditioner lattice differs");
+        if (P->nc != g_ctx->nc || P->m != g_ctx->m)
+            return set_error(QCU_ERR_INVALID, "preconditioner n_color / m_rhs differ from the context");
+    }
+    g_ctx->precond = P;
     return QCU_SUCCESS;
 }
 
@@ -579,7 +611,7 @@ int qcuGaugeFromEO(void* lex, const void* eo, const int L[4], int n_color, int p
 
 int qcuSetHopKernel(int kind) {
     clear_error();
-    if (kind != QCU_HOP_AUTO && kind != QCU_HOP_SIMT && kind != QCU_HOP_TENSOR && kind != QCU_HOP_SIMT_CS)
+    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_ACC16)
         return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
     set_hop_kind(kind);
     return QCU_SUCCESS;

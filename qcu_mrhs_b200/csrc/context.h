@@ -11,6 +11,8 @@
 
 namespace qcub {
 
+struct Precond;
+
 // Device buffer owned by the context.
 struct DevBuf {
     void* ptr = nullptr;
@@ -51,6 +53,7 @@ struct Context {
     DevBuf sv[16];
     DevBuf scalars;           // BicgScalars (device)
     BicgScalars* host_sc = nullptr;   // pinned mirror
+    Precond* precond = nullptr;       // learned preconditioner (not owned), QCU_SOLVER_PRECOND
 
     int64_t half_len() const { return g.vh * 4 * nc; }               // complex per RHS per parity
     size_t half_bytes(int prec) const { return (size_t)half_len() * m * 2 * prec_bytes(prec); }
@@ -60,8 +63,46 @@ struct Context {
     int gauge_in(int prec, const void** out);
 };
 
-// Solvers (solver.cu).  b, x: gathered full-lattice fields in FP64 ([2][Vh][4][nc][m]).
+// One Schur BiCGStab solve split into phases, so that several solves can share one
+// captured CUDA graph (solver.cu).  b, x: gathered full-lattice fields
+// ([2][Vh][4][nc][m], even half first) in the context's input precision (FP64 for
+// the mixed solver).
+//   begin()             set-up on c.stream: scalars, b', r0 = r = p = b' (synchronises once)
+//   enqueue_iteration() one BiCGStab iteration on c.stream, no host synchronisation, so
+//                       it may be captured; every kernel returns at once after `done`
+//   end()               x_e reconstruction, statistics, FP64 true residual
+class SchurSolve {
+  public:
+    SchurSolve(Context& c, bool mixed) : c_(c), mixed_(mixed) {}
+    int begin(void* x, const void* b, int max_iter, double tol);
+    int enqueue_iteration();
+    int end();
+    BicgScalars* device_scalars() const { return dsc_; }
+
+  private:
+    int begin_fused(int max_iter, double tol);
+    int begin_mixed(int max_iter, double tol);
+    Context& c_;
+    bool mixed_;
+    int P_ = 0, S_ = 0;                 // FP64/FP32 solve precision; sloppy precision
+    const void* g_ = nullptr;           // gauge in P_
+    const void* gs_ = nullptr;          // gauge in S_ (mixed)
+    char* x_ = nullptr;
+    const char* b_ = nullptr;
+    void* v_[11] = {};
+    double2* slots_ = nullptr;
+    BicgScalars* dsc_ = nullptr;
+    BicgStepArgs a_{};
+};
+
+// Whole solves (solver.cu): begin, iterations in graphs of check_interval, end.
 int solve_fused(Context& c, void* x, const void* b, int max_iter, double tol);
 int solve_mixed(Context& c, void* x, const void* b, int max_iter, double tol);
+
+// Context life cycle (api.cu), shared by the qcu.h object and the batched solver.
+int context_init(Context* c, const int L[4], int n_color, int m_rhs, int in_prec, int dslash_prec);
+void context_destroy(Context* c);
+// Copy (and cast) a caller gauge field into the context's FP64 master on c->stream.
+int context_load_gauge(Context* c, const void* gauge, int prec);
 
 }  // namespace qcub

@@ -1,0 +1,314 @@
+// dslash_h16.cu -- multi-RHS hop term for FP16 / BF16 storage in packed 16-bit arithmetic.
+//
+// Same operator, layouts and epilogues as dslash_impl.cuh (reference
+// include/kernel/su_n_m_rhs_dslash.cuh:92-105, complex_matmul.cuh:16-600).  What differs:
+//   * the 8 links of every site are read once per block, not once per (site, RHS)
+//     thread: a staging pass writes each link element W = U (forward) or U^dag
+//     (backward, with the t-boundary sign folded in) to shared memory as the pair of
+//     packed words (W.re, W.im), (-W.im, W.re), and the 8 neighbour indices next to it;
+//   * the spin projection and the link products run on packed complex numbers
+//     (one half2 / bfloat162 word = re, im): W h = (h.re, h.re) * (W.re, W.im)
+//                                               + (h.im, h.im) * (-W.im, W.re),
+//     two packed FMAs per complex multiply-add and no conversions;
+//   * each hop's result is converted to FP32 and accumulated over the 8 hops in FP32
+//     (ACC16 = false), or accumulated in the storage format (ACC16 = true, as the
+//     reference's half-precision wmma path does).
+// One thread per (half-site, RHS); the m threads of a site are consecutive.
+#include <type_traits>
+
+#include "dslash.h"
+#include "dslash_impl.cuh"
+#include "workspace.h"
+
+namespace qcub {
+
+namespace {
+
+template <typename S> struct Pk16;
+template <> struct Pk16<__half> {
+    using T2 = __half2;
+    __device__ static T2 fma(T2 a, T2 b, T2 c) { return __hfma2(a, b, c); }
+    __device__ static T2 add(T2 a, T2 b) { return __hadd2(a, b); }
+    __device__ static T2 sub(T2 a, T2 b) { return __hsub2(a, b); }
+    __device__ static float2 f32(T2 v) { return __half22float2(v); }
+};
+template <> struct Pk16<__nv_bfloat16> {
+    using T2 = __nv_bfloat162;
+    __device__ static T2 fma(T2 a, T2 b, T2 c) { return __hfma2(a, b, c); }
+    __device__ static T2 add(T2 a, T2 b) { return __hadd2(a, b); }
+    __device__ static T2 sub(T2 a, T2 b) { return __hsub2(a, b); }
+    __device__ static float2 f32(T2 v) { return __bfloat1622float2(v); }
+};
+
+template <typename T2>
+__device__ __forceinline__ uint32_t bits(T2 v) { return *reinterpret_cast<uint32_t*>(&v); }
+template <typename T2>
+__device__ __forceinline__ T2 word(uint32_t u) { return *reinterpret_cast<T2*>(&u); }
+
+// packed-word helpers (re in the low half, im in the high half; sign bit 15 / 31)
+__device__ __forceinline__ uint32_t times_i(uint32_t u) { return __byte_perm(u, 0, 0x1032) ^ 0x00008000u; }   // i v
+__device__ __forceinline__ uint32_t times_mi(uint32_t u) { return __byte_perm(u, 0, 0x1032) ^ 0x80000000u; }  // -i v
+__device__ __forceinline__ uint32_t bcast_re(uint32_t u) { return __byte_perm(u, 0, 0x1010); }
+__device__ __forceinline__ uint32_t bcast_im(uint32_t u) { return __byte_perm(u, 0, 0x3232); }
+
+constexpr int kH16Threads = 256;
+constexpr int kH16MaxSites = 32;   // sites staged per block pass
+
+template <int NC>
+struct H16Smem {
+    static constexpr int kStride = 8 * NC * NC + 1;   // uint2 per site, padded against bank conflicts
+    uint2 link[kH16MaxSites * kStride];
+    int nb[kH16MaxSites][8];
+};
+
+// half index of the neighbour of `site` (parity `parity`) along hop h = 2 mu + (backward)
+__device__ __forceinline__ int64_t h16_neighbour(const Geom& g, int64_t site, int parity, int h, bool* wrap) {
+    const SiteXYZT c = site_coords(g, (uint32_t)site);
+    const int lxh = g.lxh, Ly = g.L[1], Lz = g.L[2], Lt = g.L[3];
+    const int64_t sy = lxh, sz = (int64_t)lxh * Ly, st = sz * Lz;
+    const int mu = h >> 1;
+    const bool f = (h & 1) == 0;
+    *wrap = false;
+    if (mu == 0) {
+        const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
+        return f ? site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh)
+                 : site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1));
+    }
+    if (mu == 1) return f ? site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy) : site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
+    if (mu == 2) return f ? site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz) : site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
+    *wrap = f ? (c.t + 1 == Lt) : (c.t == 0);
+    return f ? site + (*wrap ? -(int64_t)(Lt - 1) * st : st) : site + (*wrap ? (int64_t)(Lt - 1) * st : -st);
+}
+
+// One hop of one (site, RHS): project the neighbour spinor, multiply by the staged link,
+// reconstruct into acc.  SG: sign s of gamma in this hop's projector (1 - s g or 1 + s g).
+template <int NC, typename S, bool ACC16, int MU, int SG, typename AccT>
+__device__ __forceinline__ void h16_hop(AccT (&acc)[4][NC], const uint32_t* __restrict__ psi, int m,
+                                        const uint2* __restrict__ L) {
+    using P = Pk16<S>;
+    using T2 = typename P::T2;
+    uint32_t h0[NC], h1[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const uint32_t p0 = __ldg(psi + (0 * NC + c) * m);
+        const uint32_t p1 = __ldg(psi + (1 * NC + c) * m);
+        const uint32_t p2 = __ldg(psi + (2 * NC + c) * m);
+        const uint32_t p3 = __ldg(psi + (3 * NC + c) * m);
+        if (MU == 0) {        // h0 = p0 + s i p3 ; h1 = p1 + s i p2
+            h0[c] = bits(P::add(word<T2>(p0), word<T2>(SG > 0 ? times_i(p3) : times_mi(p3))));
+            h1[c] = bits(P::add(word<T2>(p1), word<T2>(SG > 0 ? times_i(p2) : times_mi(p2))));
+        } else if (MU == 1) { // h0 = p0 - s p3 ; h1 = p1 + s p2
+            h0[c] = bits(SG > 0 ? P::sub(word<T2>(p0), word<T2>(p3)) : P::add(word<T2>(p0), word<T2>(p3)));
+            h1[c] = bits(SG > 0 ? P::add(word<T2>(p1), word<T2>(p2)) : P::sub(word<T2>(p1), word<T2>(p2)));
+        } else if (MU == 2) { // h0 = p0 + s i p2 ; h1 = p1 - s i p3
+            h0[c] = bits(P::add(word<T2>(p0), word<T2>(SG > 0 ? times_i(p2) : times_mi(p2))));
+            h1[c] = bits(P::add(word<T2>(p1), word<T2>(SG > 0 ? times_mi(p3) : times_i(p3))));
+        } else {              // h0 = p0 + s p2 ; h1 = p1 + s p3
+            h0[c] = bits(SG > 0 ? P::add(word<T2>(p0), word<T2>(p2)) : P::sub(word<T2>(p0), word<T2>(p2)));
+            h1[c] = bits(SG > 0 ? P::add(word<T2>(p1), word<T2>(p3)) : P::sub(word<T2>(p1), word<T2>(p3)));
+        }
+    }
+    uint32_t r0[NC], i0[NC], r1[NC], i1[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+        r0[k] = bcast_re(h0[k]);
+        i0[k] = bcast_im(h0[k]);
+        r1[k] = bcast_re(h1[k]);
+        i1[k] = bcast_im(h1[k]);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        T2 w0 = word<T2>(0u), w1 = word<T2>(0u);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const uint2 l = L[c * NC + k];
+            w0 = P::fma(word<T2>(r0[k]), word<T2>(l.x), w0);
+            w0 = P::fma(word<T2>(i0[k]), word<T2>(l.y), w0);
+            w1 = P::fma(word<T2>(r1[k]), word<T2>(l.x), w1);
+            w1 = P::fma(word<T2>(i1[k]), word<T2>(l.y), w1);
+        }
+        // reconstruction: acc0 += w0, acc1 += w1, acc2/acc3 from the projector
+        const uint32_t b0 = bits(w0), b1 = bits(w1);
+        uint32_t a2, a3;   // terms added to spins 2 and 3
+        if (MU == 0) {        // acc2 += -s i w1 ; acc3 += -s i w0
+            a2 = SG > 0 ? times_mi(b1) : times_i(b1);
+            a3 = SG > 0 ? times_mi(b0) : times_i(b0);
+        } else if (MU == 1) { // acc2 += s w1 ; acc3 += -s w0
+            a2 = SG > 0 ? b1 : b1 ^ 0x80008000u;
+            a3 = SG > 0 ? b0 ^ 0x80008000u : b0;
+        } else if (MU == 2) { // acc2 += -s i w0 ; acc3 += s i w1
+            a2 = SG > 0 ? times_mi(b0) : times_i(b0);
+            a3 = SG > 0 ? times_i(b1) : times_mi(b1);
+        } else {              // acc2 += s w0 ; acc3 += s w1
+            a2 = SG > 0 ? b0 : b0 ^ 0x80008000u;
+            a3 = SG > 0 ? b1 : b1 ^ 0x80008000u;
+        }
+        if constexpr (ACC16) {
+            acc[0][c] = P::add(acc[0][c], w0);
+            acc[1][c] = P::add(acc[1][c], w1);
+            acc[2][c] = P::add(acc[2][c], word<T2>(a2));
+            acc[3][c] = P::add(acc[3][c], word<T2>(a3));
+        } else {
+            const float2 f0 = P::f32(w0), f1 = P::f32(w1);
+            const float2 f2 = P::f32(word<T2>(a2)), f3 = P::f32(word<T2>(a3));
+            acc[0][c].x += f0.x; acc[0][c].y += f0.y;
+            acc[1][c].x += f1.x; acc[1][c].y += f1.y;
+            acc[2][c].x += f2.x; acc[2][c].y += f2.y;
+            acc[3][c].x += f3.x; acc[3][c].y += f3.y;
+        }
+    }
+}
+
+template <int NC, typename S, bool DAG, int EPI, bool ACC16>
+__global__ void __launch_bounds__(kH16Threads, 3) hop16_kernel(const HopParams p) {
+    using P = Pk16<S>;
+    using T2 = typename P::T2;
+    using AccT = typename std::conditional<ACC16, T2, float2>::type;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int N2 = NC * NC;
+    constexpr int SF = DAG ? 1 : -1;   // forward projector 1 - s g: sign of gamma
+    constexpr int SB = DAG ? -1 : 1;   // backward projector 1 + s g
+    __shared__ H16Smem<NC> sm;
+    if (skip_launch(p.done, p.gate)) return;
+    const int m = p.m;
+    const int spb = blockDim.x / m;
+    const int64_t vh = p.g.vh;
+    const int parity = p.parity;
+    const int64_t site_len = (int64_t)kNs * NC * m;
+    const uint32_t* __restrict__ in = static_cast<const uint32_t*>(p.in);
+    const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
+    const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
+    const int sl = threadIdx.x / m;
+    const int rhs = threadIdx.x - sl * m;
+    double2 red[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+
+    for (int64_t base = (int64_t)blockIdx.x * spb; base < vh; base += (int64_t)gridDim.x * spb) {
+        __syncthreads();   // the previous pass has finished reading the staged links
+        // neighbours of the block's sites (8 per site); the wrap flag rides in bit 31
+        for (int e = threadIdx.x; e < spb * 8; e += blockDim.x) {
+            const int s = e >> 3, h = e & 7;
+            const int64_t site = base + s;
+            if (site < vh) {
+                bool wrap;
+                const int64_t nb = h16_neighbour(p.g, site, parity, h, &wrap);
+                sm.nb[s][h] = (int)nb | (wrap ? (int)0x80000000u : 0);
+            }
+        }
+        __syncthreads();
+        // links: W = U_mu(x) forward, U_mu(x - mu)^dag backward, t-wrap sign folded in
+        for (int e = threadIdx.x; e < spb * 8 * N2; e += blockDim.x) {
+            const int s = e / (8 * N2);
+            const int rem = e - s * 8 * N2;
+            const int h = rem / N2, el = rem - h * N2;
+            const int c = el / NC, k = el - c * NC;
+            const int64_t site = base + s;
+            if (site >= vh) continue;
+            const int mu = h >> 1;
+            const int nbw = sm.nb[s][h];
+            uint32_t w;
+            if ((h & 1) == 0) {
+                w = __ldg(gauge + ((int64_t)(mu * 2 + parity) * vh + site) * N2 + c * NC + k);
+            } else {
+                const int64_t nb = nbw & 0x7fffffff;
+                w = __ldg(gauge + ((int64_t)(mu * 2 + (1 - parity)) * vh + nb) * N2 + k * NC + c) ^ 0x80000000u;
+            }
+            if (nbw < 0) w ^= tflip;
+            sm.link[s * H16Smem<NC>::kStride + h * N2 + el] = make_uint2(w, times_i(w));
+        }
+        __syncthreads();
+        const int64_t site = base + sl;
+        if (sl < spb && site < vh) {
+            AccT acc[4][NC];
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if constexpr (ACC16) acc[s][c] = word<T2>(0u);
+                    else acc[s][c] = make_float2(0.f, 0.f);
+                }
+            const uint2* L = sm.link + sl * H16Smem<NC>::kStride;
+            const int* nbs = sm.nb[sl];
+            const uint32_t* src = in + rhs;
+#define QCUB_H16_HOP(H, MU, SIGN) \
+    h16_hop<NC, S, ACC16, MU, SIGN>(acc, src + (int64_t)(nbs[H] & 0x7fffffff) * site_len, m, L + (H) * N2)
+            QCUB_H16_HOP(0, 0, SF);
+            QCUB_H16_HOP(1, 0, SB);
+            QCUB_H16_HOP(2, 1, SF);
+            QCUB_H16_HOP(3, 1, SB);
+            QCUB_H16_HOP(4, 2, SF);
+            QCUB_H16_HOP(5, 2, SB);
+            QCUB_H16_HOP(6, 3, SF);
+            QCUB_H16_HOP(7, 3, SB);
+#undef QCUB_H16_HOP
+            float2 facc[4][NC];
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if constexpr (ACC16) facc[s][c] = P::f32(acc[s][c]);
+                    else facc[s][c] = acc[s][c];
+                }
+            hop_store<NC, S, EPI, NV>(facc, p, site * site_len + rhs, red);
+        }
+    }
+    if constexpr (NV > 0) {
+        double2 rv[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        grid_reduce<NV>(rv, m, p.red);
+    }
+}
+
+template <int NC, typename S, bool ACC16>
+int launch16(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
+        return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
+    const int spb = std::min(kH16Threads / p.m, kH16MaxSites);
+    const int block = spb * p.m;
+    void (*k)(const HopParams) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop16_kernel<NC, S, true, EPI_PLAIN, ACC16> : hop16_kernel<NC, S, false, EPI_PLAIN, ACC16>; break;
+        case EPI_XPAY: k = dagger ? hop16_kernel<NC, S, true, EPI_XPAY, ACC16> : hop16_kernel<NC, S, false, EPI_XPAY, ACC16>; break;
+        case EPI_SCHUR_R0: k = hop16_kernel<NC, S, false, EPI_SCHUR_R0, ACC16>; break;
+        case EPI_SCHUR_TS: k = hop16_kernel<NC, S, false, EPI_SCHUR_TS, ACC16>; break;
+        case EPI_SCHUR: k = hop16_kernel<NC, S, false, EPI_SCHUR, ACC16>; break;
+        case EPI_RESID: k = hop16_kernel<NC, S, false, EPI_RESID, ACC16>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    const int64_t want = (p.g.vh + spb - 1) / spb;
+    int grid = resident_grid(k, block, p.g.vh * p.m);
+    if (grid > want) grid = (int)want;
+    if (grid > kScratchBlocks) grid = kScratchBlocks;   // reduction partials: one slot per block
+    k<<<grid, block, 0, st>>>(p);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
+}  // namespace
+
+bool hop16_supported(int nc, int m, int prec) {
+    return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc >= 2 && nc <= 4 && m >= 2 &&
+           m <= kH16Threads;
+}
+
+// acc16: accumulate the 8 hops in the storage format (FP16 only)
+int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, cudaStream_t st) {
+    if (!hop16_supported(nc, p.m, prec)) return set_error(QCU_ERR_UNSUPPORTED, "packed 16-bit hop: n_color %d, m %d", nc, p.m);
+    if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");
+    if (prec == QCU_PRECISION_HALF) {
+        switch (nc) {
+            case 2: return acc16 ? launch16<2, __half, true>(p, dagger, epi, st) : launch16<2, __half, false>(p, dagger, epi, st);
+            case 3: return acc16 ? launch16<3, __half, true>(p, dagger, epi, st) : launch16<3, __half, false>(p, dagger, epi, st);
+            default: return acc16 ? launch16<4, __half, true>(p, dagger, epi, st) : launch16<4, __half, false>(p, dagger, epi, st);
+        }
+    }
+    switch (nc) {
+        case 2: return launch16<2, __nv_bfloat16, false>(p, dagger, epi, st);
+        case 3: return launch16<3, __nv_bfloat16, false>(p, dagger, epi, st);
+        default: return launch16<4, __nv_bfloat16, false>(p, dagger, epi, st);
+    }
+}
+
+}  // namespace qcub

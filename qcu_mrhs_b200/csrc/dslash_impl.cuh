@@ -193,6 +193,59 @@ __device__ __forceinline__ void hop_site(typename St<S>::A2 (&acc)[4][NC], const
     }
 }
 
+// Epilogue of one (site, RHS): store out = D in (EPI_PLAIN) or the fused combination
+// with x / r0, and add this thread's terms of the fused reductions to red.
+// `base` is the offset of (site, spin 0, colour 0, RHS) in the gathered layout.
+template <int NC, typename S, int EPI, int NV>
+__device__ __forceinline__ void hop_store(const typename St<S>::A2 (&acc)[4][NC], const HopParams& p,
+                                          int64_t base, double2 (&red)[NV > 0 ? NV : 1]) {
+    using S2 = typename St<S>::S2;
+    using A = typename St<S>::A;
+    using A2 = typename St<S>::A2;
+    const int m = p.m;
+    S2* __restrict__ out = static_cast<S2*>(p.out);
+    const S2* __restrict__ xv = static_cast<const S2*>(p.x);
+    const S2* __restrict__ r0 = static_cast<const S2*>(p.r0);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int64_t o = base + (int64_t)(s * NC + c) * m;
+            A2 v = acc[s][c];
+            if (EPI == EPI_PLAIN) {
+                out[o] = St<S>::cv(v);
+            } else {
+                const A2 xx = St<S>::ld(xv[o]);
+                const A a = (A)p.a;
+                A2 res;
+                if (EPI == EPI_XPAY) {
+                    res = mk2<A2>(xx.x + a * v.x, xx.y + a * v.y);
+                } else if (EPI == EPI_RESID) {
+                    const A2 yy = St<S>::ld(r0[o]);
+                    res = mk2<A2>(yy.x - xx.x + a * v.x, yy.y - xx.y + a * v.y);
+                } else {
+                    res = mk2<A2>(xx.x - a * v.x, xx.y - a * v.y);
+                }
+                const S2 rs = St<S>::cv(res);
+                out[o] = rs;
+                if (NV > 0) {
+                    const A2 rr = St<S>::ld(rs);
+                    if (EPI == EPI_RESID) {
+                        red[0].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                    } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
+                        const A2 q = St<S>::ld(r0[o]);
+                        red[0].x += (double)q.x * rr.x + (double)q.y * rr.y;
+                        red[0].y += (double)q.x * rr.y - (double)q.y * rr.x;
+                    } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
+                        red[0].x += (double)rr.x * xx.x + (double)rr.y * xx.y;
+                        red[0].y += (double)rr.x * xx.y - (double)rr.y * xx.x;
+                        red[NV - 1].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                    }
+                }
+            }
+        }
+}
+
 // Minimum resident blocks per SM requested from the register allocator: FP64 at small N
 // otherwise takes ~190 registers (one block per SM, latency-bound); capping it at 128
 // doubles the warps in flight.  Large N keeps the compiler's choice (accumulators dominate).
@@ -213,9 +266,6 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
     const int64_t total = p.g.vh * m;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t site_len = (int64_t)kNs * NC * m;
-    S2* __restrict__ out = static_cast<S2*>(p.out);
-    const S2* __restrict__ xv = static_cast<const S2*>(p.x);
-    const S2* __restrict__ r0 = static_cast<const S2*>(p.r0);
     double2 red[NV > 0 ? NV : 1];
 #pragma unroll
     for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
@@ -228,45 +278,7 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
          site += site_stride) {
         A2 acc[4][NC];
         hop_site<NC, S, DAG>(acc, p, site, rhs);
-        const int64_t base = site * site_len + rhs;
-#pragma unroll
-        for (int s = 0; s < 4; ++s)
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const int64_t o = base + (int64_t)(s * NC + c) * m;
-                A2 v = acc[s][c];
-                if (EPI == EPI_PLAIN) {
-                    out[o] = St<S>::cv(v);
-                } else {
-                    const A2 xx = St<S>::ld(xv[o]);
-                    const A a = (A)p.a;
-                    A2 res;
-                    if (EPI == EPI_XPAY) {
-                        res = mk2<A2>(xx.x + a * v.x, xx.y + a * v.y);
-                    } else if (EPI == EPI_RESID) {
-                        const A2 yy = St<S>::ld(r0[o]);
-                        res = mk2<A2>(yy.x - xx.x + a * v.x, yy.y - xx.y + a * v.y);
-                    } else {
-                        res = mk2<A2>(xx.x - a * v.x, xx.y - a * v.y);
-                    }
-                    const S2 rs = St<S>::cv(res);
-                    out[o] = rs;
-                    if (NV > 0) {
-                        const A2 rr = St<S>::ld(rs);
-                        if (EPI == EPI_RESID) {
-                            red[0].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
-                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
-                            const A2 q = St<S>::ld(r0[o]);
-                            red[0].x += (double)q.x * rr.x + (double)q.y * rr.y;
-                            red[0].y += (double)q.x * rr.y - (double)q.y * rr.x;
-                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
-                            red[0].x += (double)rr.x * xx.x + (double)rr.y * xx.y;
-                            red[0].y += (double)rr.x * xx.y - (double)rr.y * xx.x;
-                            red[NV - 1].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
-                        }
-                    }
-                }
-            }
+        hop_store<NC, S, EPI, NV>(acc, p, site * site_len + rhs, red);
     }
     if constexpr (NV > 0) {
         double2 rv[NV];

@@ -121,9 +121,11 @@ bool hop_tc_supported(int nc, int m, int prec);
 
 // Kernel used when the selection is AUTO: the tuned choice for (n_color, m, precision)
 // if one was recorded (qcuTuneHop / the tuning cache), else a static rule: colour-split
-// SIMT for FP64 and for N >= 5 (fewer registers), per-(site, RHS) SIMT otherwise.
+// SIMT for N >= 5 (fewer registers per thread), per-(site, RHS) SIMT otherwise.
 int auto_hop_kind(int nc, int m, int prec);
 int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
+bool hop16_supported(int nc, int m, int prec);
+int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, cudaStream_t st);
 
 // ---------------- hop dispatch ----------------
 template <typename S>
@@ -150,6 +152,9 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec) &&
         reinterpret_cast<uintptr_t>(p.in) % 16 == 0)
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
+    if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16) && hop16_supported(nc, p.m, prec))
+        return hop16_launch(p, nc, prec, dagger, epi, kind == QCU_HOP_PACKED16_ACC16 && prec == QCU_PRECISION_HALF,
+                            st);
     const bool cs = (kind == QCU_HOP_SIMT_CS) && nc * p.m <= kRedThreads;
     return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st, cs); });
 }

@@ -21,6 +21,7 @@
 #include "blas.h"
 #include "context.h"
 #include "dslash.h"
+#include "precond.h"
 
 namespace qcub {
 
@@ -156,147 +157,254 @@ int finish_stats(Context& c, int prec, const void* gauge, const void* x, const v
 
 }  // namespace
 
-int solve_fused(Context& c, void* x, const void* b, int max_iter, double tol) {
-    const int P = c.in_prec;
-    if (P != QCU_PRECISION_DOUBLE && P != QCU_PRECISION_SINGLE)
+int SchurSolve::begin(void* x, const void* b, int max_iter, double tol) {
+    x_ = static_cast<char*>(x);
+    b_ = static_cast<const char*>(b);
+    dsc_ = static_cast<BicgScalars*>(c_.scalars.ptr);
+    return mixed_ ? begin_mixed(max_iter, tol) : begin_fused(max_iter, tol);
+}
+
+int SchurSolve::begin_fused(int max_iter, double tol) {
+    Context& c = c_;
+    P_ = c.in_prec;
+    if (P_ != QCU_PRECISION_DOUBLE && P_ != QCU_PRECISION_SINGLE)
         return set_error(QCU_ERR_UNSUPPORTED, "the solve precision must be double or single");
-    const void* gauge = nullptr;
-    int rc = c.gauge_in(P, &gauge);
+    int rc = c.gauge_in(P_, &g_);
     if (rc) return rc;
-    const size_t hb = c.half_bytes(P);
-    for (int i = 0; i < 8; ++i)
+    const size_t hb = c.half_bytes(P_);
+    for (int i = 0; i < 8; ++i) {
         if ((rc = c.sv[i].ensure(hb))) return rc;
+        v_[i] = c.sv[i].ptr;
+    }
     if ((rc = c.sv[15].ensure(sizeof(double2) * 8 * kMaxRhs))) return rc;
-    void* bp = c.sv[0].ptr; void* r0 = c.sv[1].ptr; void* r = c.sv[2].ptr; void* p = c.sv[3].ptr;
-    void* v = c.sv[4].ptr; void* s = c.sv[5].ptr; void* t = c.sv[6].ptr; void* tmp = c.sv[7].ptr;
-    double2* slots = static_cast<double2*>(c.sv[15].ptr);
-    BicgScalars* dsc = static_cast<BicgScalars*>(c.scalars.ptr);
-    const char* be = static_cast<const char*>(b);
-    const void* bo = be + hb;
-    char* xe = static_cast<char*>(x);
-    void* xo = xe + hb;
+    slots_ = static_cast<double2*>(c.sv[15].ptr);
+    void* bp = v_[0];
+    const void* be = b_;
+    const void* bo = b_ + hb;
     const int64_t len = c.half_len();
-    const double k2 = c.kappa * c.kappa;
-    Hop hop{c, P, gauge};
+    Hop hop{c, P_, g_};
 
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev0, c.stream));
-    if ((rc = prepare_scalars(c, dsc, max_iter, tol, 0))) return rc;
+    if ((rc = prepare_scalars(c, dsc_, max_iter, tol, 0))) return rc;
     // b' = b_o + kappa D_oe b_e
     if ((rc = hop.launch(bp, be, 1, EPI_XPAY, bo, nullptr, c.kappa))) return rc;
-    BicgStepArgs a;
-    a.src = bp; a.r0 = r0; a.r = r; a.p = p; a.v = v; a.s = s; a.t = t; a.x = xo;
-    a.sc = dsc; a.ws = c.ws; a.len = len; a.m = c.m;
-    if ((rc = bicg_step(STEP_INIT, P, P, a, c.stream))) return rc;
+    BicgStepArgs& a = a_;
+    a.src = bp; a.r0 = v_[1]; a.r = v_[2]; a.p = v_[3]; a.v = v_[4]; a.s = v_[5]; a.t = v_[6];
+    a.x = x_ + hb;
+    a.sc = dsc_; a.ws = c.ws; a.len = len; a.m = c.m;
+    if ((rc = bicg_step(STEP_INIT, P_, P_, a, c.stream))) return rc;
     // full-system norms of b (stopping reference with stop_true_residual)
-    if ((rc = mrhs_dotc(slots + 4 * kMaxRhs, be, be, len, c.m, P, c.ws, c.stream))) return rc;
-    if ((rc = mrhs_dotc(slots + 5 * kMaxRhs, bo, bo, len, c.m, P, c.ws, c.stream))) return rc;
-    set_bfull_kernel<<<1, 64, 0, c.stream>>>(dsc, slots + 4 * kMaxRhs, slots + 5 * kMaxRhs, c.m,
+    if ((rc = mrhs_dotc(slots_ + 4 * kMaxRhs, be, be, len, c.m, P_, c.ws, c.stream))) return rc;
+    if ((rc = mrhs_dotc(slots_ + 5 * kMaxRhs, bo, bo, len, c.m, P_, c.ws, c.stream))) return rc;
+    set_bfull_kernel<<<1, 64, 0, c.stream>>>(dsc_, slots_ + 4 * kMaxRhs, slots_ + 5 * kMaxRhs, c.m,
                                              c.opts.stop_true_residual ? 1 : 0);
     QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
 
-    const int* done = &dsc->done;
-    auto iteration = [&]() -> int {
-        int e;
+int SchurSolve::begin_mixed(int max_iter, double tol) {
+    Context& c = c_;
+    if (c.in_prec != QCU_PRECISION_DOUBLE)
+        return set_error(QCU_ERR_UNSUPPORTED, "mixed precision needs double-precision fields");
+    S_ = c.opts.sloppy_precision;
+    if (S_ != QCU_PRECISION_SINGLE && S_ != QCU_PRECISION_HALF && S_ != QCU_PRECISION_BF16)
+        return set_error(QCU_ERR_INVALID, "sloppy precision %d (single, half or bf16)", S_);
+    P_ = QCU_PRECISION_DOUBLE;
+    int rc;
+    if ((rc = c.gauge_in(P_, &g_))) return rc;
+    if ((rc = c.gauge_in(S_, &gs_))) return rc;
+    const size_t hb = c.half_bytes(P_);
+    const size_t hs = c.half_bytes(S_);
+    const size_t he = c.half_bytes(QCU_PRECISION_SINGLE);
+    for (int i = 0; i < 11; ++i) {
+        if ((rc = c.sv[i].ensure(i < 3 ? hb : (i < 10 ? hs : he)))) return rc;
+        v_[i] = c.sv[i].ptr;
+    }
+    if ((rc = c.sv[15].ensure(sizeof(double2) * 8 * kMaxRhs))) return rc;
+    slots_ = static_cast<double2*>(c.sv[15].ptr);
+    // v_: 0 b', 1 r64, 2 tmp64, 3 r0s, 4 rs, 5 ps, 6 vs, 7 ss, 8 ts, 9 tmps, 10 e (FP32)
+    void* bp = v_[0];
+    void* r64 = v_[1];
+    const void* be = b_;
+    const void* bo = b_ + hb;
+    void* xo = x_ + hb;
+    const int64_t len = c.half_len();
+    Hop h64{c, P_, g_};
+
+    QCUB_CUDA_CHECK(cudaEventRecord(c.ev0, c.stream));
+    if ((rc = prepare_scalars(c, dsc_, max_iter, tol, 1))) return rc;
+    // b' = b_o + kappa D_oe b_e (FP64); ||b||^2 of the full system
+    if ((rc = h64.launch(bp, be, 1, EPI_XPAY, bo, nullptr, c.kappa))) return rc;
+    if ((rc = mrhs_dotc(slots_ + 4 * kMaxRhs, be, be, len, c.m, P_, c.ws, c.stream))) return rc;
+    if ((rc = mrhs_dotc(slots_ + 5 * kMaxRhs, bo, bo, len, c.m, P_, c.ws, c.stream))) return rc;
+    set_bfull_kernel<<<1, 64, 0, c.stream>>>(dsc_, slots_ + 4 * kMaxRhs, slots_ + 5 * kMaxRhs, c.m, 1);
+    QCUB_CHECK_LAUNCH();
+    // x_o = 0, r64 = b', e = 0, rtrue2 = ||b'||^2
+    QCUB_CUDA_CHECK(cudaMemsetAsync(xo, 0, hb, c.stream));
+    QCUB_CUDA_CHECK(cudaMemsetAsync(v_[10], 0, he, c.stream));
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(r64, bp, hb, cudaMemcpyDeviceToDevice, c.stream));
+    if ((rc = mrhs_norm(nullptr, r64, len, c.m, P_, c.ws, c.stream, FIN_RNORM, dsc_))) return rc;
+    if ((rc = mp_update(dsc_, c.m, 1, c.stream))) return rc;
+    if ((rc = mp_load(S_, v_[4], v_[5], v_[3], r64, dsc_, len, c.m, 1, c.ws, c.stream))) return rc;
+    BicgStepArgs& a = a_;
+    a.r0 = v_[3]; a.r = v_[4]; a.p = v_[5]; a.v = v_[6]; a.s = v_[7]; a.t = v_[8]; a.x = v_[10];
+    a.sc = dsc_; a.ws = c.ws; a.len = len; a.m = c.m;
+    return QCU_SUCCESS;
+}
+
+int SchurSolve::enqueue_iteration() {
+    Context& c = c_;
+    const double k2 = c.kappa * c.kappa;
+    const int* done = &dsc_->done;
+    int e;
+    if (!mixed_) {
+        void* r0 = v_[1]; void* p = v_[3]; void* v = v_[4]; void* s = v_[5]; void* t = v_[6];
+        void* tmp = v_[7];
+        Hop hop{c, P_, g_};
         if ((e = hop.launch(tmp, p, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
-        if ((e = hop.launch(v, tmp, 1, EPI_SCHUR_R0, p, r0, k2, FIN_ALPHA, dsc, dsc->red[0], done))) return e;
-        if ((e = bicg_step(STEP_S, P, P, a, c.stream))) return e;
+        if ((e = hop.launch(v, tmp, 1, EPI_SCHUR_R0, p, r0, k2, FIN_ALPHA, dsc_, dsc_->red[0], done))) return e;
+        if ((e = bicg_step(STEP_S, P_, P_, a_, c.stream))) return e;
         if ((e = hop.launch(tmp, s, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
-        if ((e = hop.launch(t, tmp, 1, EPI_SCHUR_TS, s, nullptr, k2, FIN_OMEGA, dsc, dsc->red[0], done))) return e;
-        if ((e = bicg_step(STEP_XR, P, P, a, c.stream))) return e;
-        return bicg_step(STEP_P, P, P, a, c.stream);
-    };
-    const int interval = c.opts.check_interval > 0 ? c.opts.check_interval : 8;
-    cudaGraphExec_t exec = nullptr;
-    if ((rc = capture(c, interval, iteration, &exec))) return rc;
-    rc = run_graph(c, exec, dsc);
-    cudaGraphExecDestroy(exec);
-    if (rc) return rc;
+        if ((e = hop.launch(t, tmp, 1, EPI_SCHUR_TS, s, nullptr, k2, FIN_OMEGA, dsc_, dsc_->red[0], done))) return e;
+        if ((e = bicg_step(STEP_XR, P_, P_, a_, c.stream))) return e;
+        return bicg_step(STEP_P, P_, P_, a_, c.stream);
+    }
+    void* bp = v_[0]; void* r64 = v_[1]; void* tmp64 = v_[2];
+    void* r0s = v_[3]; void* rs = v_[4]; void* ps = v_[5]; void* vs = v_[6]; void* ss = v_[7];
+    void* ts = v_[8]; void* tmps = v_[9]; void* ev = v_[10];
+    void* xo = x_ + c.half_bytes(P_);
+    const int64_t len = c.half_len();
+    const int* gate = &dsc_->gate;
+    const int XP = QCU_PRECISION_SINGLE;
+    Hop h64{c, P_, g_};
+    Hop hs{c, S_, gs_};
+    // sloppy BiCGStab iteration
+    if ((e = hs.launch(tmps, ps, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
+    if ((e = hs.launch(vs, tmps, 1, EPI_SCHUR_R0, ps, r0s, k2, FIN_ALPHA, dsc_, dsc_->red[0], done))) return e;
+    if ((e = bicg_step(STEP_S, S_, XP, a_, c.stream))) return e;
+    if ((e = hs.launch(tmps, ss, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
+    if ((e = hs.launch(ts, tmps, 1, EPI_SCHUR_TS, ss, nullptr, k2, FIN_OMEGA, dsc_, dsc_->red[0], done))) return e;
+    if ((e = bicg_step(STEP_XR, S_, XP, a_, c.stream))) return e;
+    if ((e = bicg_step(STEP_P, S_, XP, a_, c.stream))) return e;
+    // reliable update (every kernel returns at once unless one is pending)
+    if ((e = mp_accum(xo, ev, dsc_, len, c.m, c.stream))) return e;
+    if ((e = h64.launch(tmp64, xo, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done, gate))) return e;
+    if ((e = h64.launch(r64, tmp64, 1, EPI_RESID, xo, bp, k2, FIN_RNORM, dsc_, slots_ + 6 * kMaxRhs, done, gate))) return e;
+    if ((e = mp_update(dsc_, c.m, 0, c.stream))) return e;
+    return mp_load(S_, rs, ps, r0s, r64, dsc_, len, c.m, 0, c.ws, c.stream);
+}
+
+int SchurSolve::end() {
+    Context& c = c_;
+    int rc;
+    const size_t hb = c.half_bytes(P_);
+    void* tmp = mixed_ ? v_[2] : v_[7];
+    // final device scalars (iterations, status, norms) for the statistics
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(c.host_sc, dsc_, sizeof(BicgScalars), cudaMemcpyDeviceToHost, c.stream));
+    QCUB_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    Hop hop{c, P_, g_};
     // x_e = b_e + kappa D_eo x_o
-    if ((rc = hop.launch(xe, xo, 0, EPI_XPAY, be, nullptr, c.kappa))) return rc;
+    if ((rc = hop.launch(x_, x_ + hb, 0, EPI_XPAY, b_, nullptr, c.kappa))) return rc;
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev1, c.stream));
-    if ((rc = finish_stats(c, P, gauge, x, b, tmp, slots))) return rc;
+    if ((rc = finish_stats(c, P_, g_, x_, b_, tmp, slots_))) return rc;
+    if (mixed_)
+        for (int j = 0; j < c.m; ++j) {
+            const double b2 = c.host_sc->bfull2[j];
+            c.stats.recursive_residual[j] = b2 > 0 ? std::sqrt(c.host_sc->rtrue2[j] / b2) : 0.0;
+        }
     float ms = 0.f;
     QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.solve_seconds = ms * 1e-3;
     if (c.stats.status != QCU_SUCCESS)
-        return set_error(c.stats.status, "BiCGStab stopped after %d iterations (%s)", c.stats.iterations,
+        return set_error(c.stats.status, "%sBiCGStab stopped after %d iterations (%s)", mixed_ ? "mixed " : "",
+                         c.stats.iterations,
                          c.stats.status == QCU_ERR_BREAKDOWN ? "breakdown" : "max_iteration reached");
     return QCU_SUCCESS;
 }
 
+namespace {
+
+int solve_one(Context& c, void* x, const void* b, int max_iter, double tol, bool mixed) {
+    SchurSolve solve(c, mixed);
+    int rc = solve.begin(x, b, max_iter, tol);
+    if (rc) return rc;
+    const int interval = c.opts.check_interval > 0 ? c.opts.check_interval : 8;
+    cudaGraphExec_t exec = nullptr;
+    if ((rc = capture(c, interval, [&]() { return solve.enqueue_iteration(); }, &exec))) return rc;
+    rc = run_graph(c, exec, solve.device_scalars());
+    cudaGraphExecDestroy(exec);
+    if (rc) return rc;
+    return solve.end();
+}
+
+}  // namespace
+
+int solve_fused(Context& c, void* x, const void* b, int max_iter, double tol) {
+    return solve_one(c, x, b, max_iter, tol, false);
+}
+
 int solve_mixed(Context& c, void* x, const void* b, int max_iter, double tol) {
+    return solve_one(c, x, b, max_iter, tol, true);
+}
+
+// Right-preconditioned BiCGStab on the full system M (P y) = b, x = P y, in FP64 with P
+// applied in FP32 (x and r are updated with the P outputs actually computed, so the
+// recursive residual stays the FP64 residual of x whatever P's rounding).  Stops when
+// every RHS has ||r_j|| <= tol ||b_j|| on the full system.  When it breaks down or hits
+// max_iter, the plain FP64 Schur BiCGStab solves the system instead.
+int solve_precond(Context& c, Precond* P, void* x, const void* b, int max_iter, double tol) {
+    if (!P) return set_error(QCU_ERR_STATE, "no preconditioner attached (qcuSetPreconditioner)");
     if (c.in_prec != QCU_PRECISION_DOUBLE)
-        return set_error(QCU_ERR_UNSUPPORTED, "mixed precision needs double-precision fields");
-    const int S = c.opts.sloppy_precision;
-    if (S != QCU_PRECISION_SINGLE && S != QCU_PRECISION_HALF && S != QCU_PRECISION_BF16)
-        return set_error(QCU_ERR_INVALID, "sloppy precision %d (single, half or bf16)", S);
-    const int D = QCU_PRECISION_DOUBLE;
+        return set_error(QCU_ERR_UNSUPPORTED, "the preconditioned solve needs double-precision fields");
+    for (int i = 0; i < 4; ++i)
+        if (P->g.L[i] != c.g.L[i]) return set_error(QCU_ERR_INVALID, "preconditioner lattice differs");
+    if (P->nc != c.nc || P->m != c.m) return set_error(QCU_ERR_INVALID, "preconditioner n_color / m_rhs differ");
+    if (P->t_sign != c.opts.t_boundary) return set_error(QCU_ERR_INVALID, "preconditioner t boundary differs");
+    const int D = QCU_PRECISION_DOUBLE, F = QCU_PRECISION_SINGLE;
     const void* g64 = nullptr;
-    const void* gs = nullptr;
+    const void* g32 = nullptr;
     int rc;
-    if ((rc = c.gauge_in(D, &g64))) return rc;
-    if ((rc = c.gauge_in(S, &gs))) return rc;
-    const size_t hb = c.half_bytes(D);
-    const size_t hs = c.half_bytes(S);
-    const size_t he = c.half_bytes(QCU_PRECISION_SINGLE);
-    for (int i = 0; i < 3; ++i)
-        if ((rc = c.sv[i].ensure(hb))) return rc;
-    for (int i = 3; i < 10; ++i)
-        if ((rc = c.sv[i].ensure(hs))) return rc;
-    if ((rc = c.sv[10].ensure(he))) return rc;
+    if ((rc = c.gauge_in(D, &g64)) || (rc = c.gauge_in(F, &g32))) return rc;
+    const size_t fb = 2 * c.half_bytes(D), ff = 2 * c.half_bytes(F);
+    void* v_[10];
+    for (int i = 0; i < 10; ++i) {
+        if ((rc = c.sv[i].ensure(i < 8 ? fb : ff))) return rc;
+        v_[i] = c.sv[i].ptr;
+    }
     if ((rc = c.sv[15].ensure(sizeof(double2) * 8 * kMaxRhs))) return rc;
-    void* bp = c.sv[0].ptr; void* r64 = c.sv[1].ptr; void* tmp64 = c.sv[2].ptr;
-    void* r0s = c.sv[3].ptr; void* rs = c.sv[4].ptr; void* ps = c.sv[5].ptr; void* vs = c.sv[6].ptr;
-    void* ss = c.sv[7].ptr; void* ts = c.sv[8].ptr; void* tmps = c.sv[9].ptr; void* e = c.sv[10].ptr;
     double2* slots = static_cast<double2*>(c.sv[15].ptr);
+    void* r0 = v_[0]; void* r = v_[1]; void* p = v_[2]; void* v = v_[3]; void* s = v_[4]; void* t = v_[5];
+    void* ph = v_[6]; void* sh = v_[7];
+    float2* fin = static_cast<float2*>(v_[8]);
+    float2* fout = static_cast<float2*>(v_[9]);
     BicgScalars* dsc = static_cast<BicgScalars*>(c.scalars.ptr);
-    const char* be = static_cast<const char*>(b);
-    const void* bo = be + hb;
-    char* xe = static_cast<char*>(x);
-    void* xo = xe + hb;
-    const int64_t len = c.half_len();
-    const double k2 = c.kappa * c.kappa;
-    Hop h64{c, D, g64};
-    Hop hs_{c, S, gs};
+    const int64_t len = 2 * c.half_len();
+    const int64_t n = len * c.m;
+    const int* done = &dsc->done;
 
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev0, c.stream));
-    if ((rc = prepare_scalars(c, dsc, max_iter, tol, 1))) return rc;
-    // b' = b_o + kappa D_oe b_e (FP64); ||b||^2 of the full system
-    if ((rc = h64.launch(bp, be, 1, EPI_XPAY, bo, nullptr, c.kappa))) return rc;
-    if ((rc = mrhs_dotc(slots + 4 * kMaxRhs, be, be, len, c.m, D, c.ws, c.stream))) return rc;
-    if ((rc = mrhs_dotc(slots + 5 * kMaxRhs, bo, bo, len, c.m, D, c.ws, c.stream))) return rc;
-    set_bfull_kernel<<<1, 64, 0, c.stream>>>(dsc, slots + 4 * kMaxRhs, slots + 5 * kMaxRhs, c.m, 1);
-    QCUB_CHECK_LAUNCH();
-    // x_o = 0, r64 = b', e = 0, rtrue2 = ||b'||^2
-    QCUB_CUDA_CHECK(cudaMemsetAsync(xo, 0, hb, c.stream));
-    QCUB_CUDA_CHECK(cudaMemsetAsync(e, 0, he, c.stream));
-    QCUB_CUDA_CHECK(cudaMemcpyAsync(r64, bp, hb, cudaMemcpyDeviceToDevice, c.stream));
-    if ((rc = mrhs_norm(nullptr, r64, len, c.m, D, c.ws, c.stream, FIN_RNORM, dsc))) return rc;
-    if ((rc = mp_update(dsc, c.m, 1, c.stream))) return rc;
-    if ((rc = mp_load(S, rs, ps, r0s, r64, dsc, len, c.m, 1, c.ws, c.stream))) return rc;
-
+    if ((rc = prepare_scalars(c, dsc, max_iter, tol, 0))) return rc;
     BicgStepArgs a;
-    a.r0 = r0s; a.r = rs; a.p = ps; a.v = vs; a.s = ss; a.t = ts; a.x = e;
+    a.src = const_cast<void*>(b); a.r0 = r0; a.r = r; a.p = p; a.v = v; a.s = s; a.t = t; a.x = x;
     a.sc = dsc; a.ws = c.ws; a.len = len; a.m = c.m;
-    const int* done = &dsc->done;
-    const int* gate = &dsc->gate;
-    const int XP = QCU_PRECISION_SINGLE;
+    if ((rc = bicg_step(STEP_INIT, D, D, a, c.stream))) return rc;
+    auto precondition = [&](void* out64, const void* in64) -> int {
+        int e;
+        if ((e = pc_cast(fin, F, in64, D, n, done, c.stream))) return e;
+        if ((e = P->apply(fout, fin, g32, c.stream, done))) return e;
+        return pc_cast(out64, D, fout, F, n, done, c.stream);
+    };
     auto iteration = [&]() -> int {
-        int q;
-        // sloppy BiCGStab iteration
-        if ((q = hs_.launch(tmps, ps, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return q;
-        if ((q = hs_.launch(vs, tmps, 1, EPI_SCHUR_R0, ps, r0s, k2, FIN_ALPHA, dsc, dsc->red[0], done))) return q;
-        if ((q = bicg_step(STEP_S, S, XP, a, c.stream))) return q;
-        if ((q = hs_.launch(tmps, ss, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return q;
-        if ((q = hs_.launch(ts, tmps, 1, EPI_SCHUR_TS, ss, nullptr, k2, FIN_OMEGA, dsc, dsc->red[0], done))) return q;
-        if ((q = bicg_step(STEP_XR, S, XP, a, c.stream))) return q;
-        if ((q = bicg_step(STEP_P, S, XP, a, c.stream))) return q;
-        // reliable update (every kernel returns at once unless one is pending)
-        if ((q = mp_accum(xo, e, dsc, len, c.m, c.stream))) return q;
-        if ((q = h64.launch(tmp64, xo, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done, gate))) return q;
-        if ((q = h64.launch(r64, tmp64, 1, EPI_RESID, xo, bp, k2, FIN_RNORM, dsc, slots + 6 * kMaxRhs, done, gate))) return q;
-        if ((q = mp_update(dsc, c.m, 0, c.stream))) return q;
-        return mp_load(S, rs, ps, r0s, r64, dsc, len, c.m, 0, c.ws, c.stream);
+        int e;
+        if ((e = precondition(ph, p))) return e;
+        if ((e = full_mat(v, ph, g64, c.g, c.nc, c.m, c.kappa, c.opts.t_boundary, false, D, c.stream, done))) return e;
+        if ((e = pc_alpha(r0, v, dsc, len, c.m, c.ws, c.stream))) return e;
+        if ((e = bicg_step(STEP_S, D, D, a, c.stream))) return e;
+        if ((e = precondition(sh, s))) return e;
+        if ((e = full_mat(t, sh, g64, c.g, c.nc, c.m, c.kappa, c.opts.t_boundary, false, D, c.stream, done))) return e;
+        if ((e = pc_omega(t, s, dsc, len, c.m, c.ws, c.stream))) return e;
+        if ((e = pc_xr(x, r, ph, sh, s, t, r0, dsc, len, c.m, c.ws, c.stream))) return e;
+        return bicg_step(STEP_P, D, D, a, c.stream);
     };
     const int interval = c.opts.check_interval > 0 ? c.opts.check_interval : 8;
     cudaGraphExec_t exec = nullptr;
@@ -304,22 +412,22 @@ int solve_mixed(Context& c, void* x, const void* b, int max_iter, double tol) {
     rc = run_graph(c, exec, dsc);
     cudaGraphExecDestroy(exec);
     if (rc) return rc;
-    // x_e = b_e + kappa D_eo x_o (FP64)
-    if ((rc = h64.launch(xe, xo, 0, EPI_XPAY, be, nullptr, c.kappa))) return rc;
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev1, c.stream));
-    if ((rc = finish_stats(c, D, g64, x, b, tmp64, slots))) return rc;
-    for (int j = 0; j < c.m; ++j) {
-        const double b2 = c.host_sc->bfull2[j];
-        c.stats.recursive_residual[j] = b2 > 0 ? std::sqrt(c.host_sc->rtrue2[j] / b2) : 0.0;
-    }
+    if ((rc = finish_stats(c, D, g64, x, b, v, slots))) return rc;
     float ms = 0.f;
     QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.solve_seconds = ms * 1e-3;
-    if (c.stats.status != QCU_SUCCESS)
-        return set_error(c.stats.status, "mixed BiCGStab stopped after %d iterations (%s)",
-                         c.stats.iterations,
-                         c.stats.status == QCU_ERR_BREAKDOWN ? "breakdown" : "max_iteration reached");
-    return QCU_SUCCESS;
+    c.stats.precond_iterations = c.stats.iterations;
+    if (c.stats.status == QCU_SUCCESS) return QCU_SUCCESS;
+    // fallback: the plain FP64 Schur BiCGStab from scratch
+    const int pit = c.stats.iterations;
+    const double pre_seconds = c.stats.solve_seconds;
+    c.stats = QcuSolveStats{};
+    rc = solve_fused(c, x, b, max_iter, tol);
+    c.stats.fallback = 1;
+    c.stats.precond_iterations = pit;
+    c.stats.solve_seconds += pre_seconds;
+    return rc;
 }
 
 }  // namespace qcub

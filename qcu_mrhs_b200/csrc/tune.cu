@@ -10,6 +10,7 @@
 namespace qcub {
 
 bool hop_tc_supported(int nc, int m, int prec);
+bool hop16_supported(int nc, int m, int prec);
 void set_hop_kind(int k);
 int hop_kind();
 
@@ -58,7 +59,7 @@ int auto_hop_kind(int nc, int m, int prec) {
         auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
         if (it != g_tuned.end()) return it->second;
     }
-    if (prec == QCU_PRECISION_DOUBLE || nc >= 5) return nc * m <= kRedThreads ? QCU_HOP_SIMT_CS : QCU_HOP_SIMT;
+    if (nc >= 5) return nc * m <= kRedThreads ? QCU_HOP_SIMT_CS : QCU_HOP_SIMT;
     return QCU_HOP_SIMT;
 }
 
@@ -96,12 +97,15 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
     fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(in), (int64_t)(spin_bytes / 4), 1u);
     fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(gauge), (int64_t)(gauge_bytes / 4), 2u);
     const int saved = hop_kind();
-    int kinds[3] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR};
+    // PACKED16_ACC16 is not a candidate: it trades accuracy for speed, so only an explicit
+    // request selects it
+    int kinds[4] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16};
     int best = QCU_HOP_SIMT;
     float best_ms = 1e30f;
     for (int kind : kinds) {
         if (kind == QCU_HOP_SIMT_CS && nc * m > kRedThreads) continue;
         if (kind == QCU_HOP_TENSOR && !hop_tc_supported(nc, m, prec)) continue;
+        if (kind == QCU_HOP_PACKED16 && !hop16_supported(nc, m, prec)) continue;
         set_hop_kind(kind);
         HopParams p{};
         p.in = in;

@@ -15,6 +15,7 @@ import ctypes
 import json
 
 PRECS = {"f64": 2, "f32": 1, "f16": 0, "bf16": 4}
+KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16"]
 
 
 def hop_bytes(vh, nc, m, s):
@@ -56,7 +57,7 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
     dur = e0.elapsed_time(e1) / 1e3 / reps
     s = q.PREC_BYTES[prec]
     q.check(lib.qcuSetHopKernel(0))
-    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "kernel": ["auto", "simt", "tcgen05"][kernel],
+    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "kernel": KERNELS[kernel],
             "launch_us": dur * 1e6,
             "GBps": hop_bytes(vh, nc, m, s) / dur / 1e9, "GFLOPs": hop_flops(vh, nc, m) / dur / 1e9,
             "algorithmic_bytes": hop_bytes(vh, nc, m, s)}
@@ -70,10 +71,10 @@ def main():
     ap.add_argument("--prec", nargs="+", default=["bf16", "f64"])
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--kernel", nargs="+", default=["auto"], choices=["auto", "simt", "tcgen05"])
+    ap.add_argument("--kernel", nargs="+", default=["auto"], choices=KERNELS)
     args = ap.parse_args()
     for kname in args.kernel:
-        kern = {"auto": 0, "simt": 1, "tcgen05": 2}[kname]
+        kern = KERNELS.index(kname)
         for p in args.prec:
             print(json.dumps(run(tuple(args.L), args.nc, args.m, p, args.reps, args.warmup, kernel=kern)),
                   flush=True)

@@ -146,6 +146,25 @@ def test_mixed_precision_reaches_fp64_true_residual(oracle_lib, sloppy):
     assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-2, atol=1e-15)
 
 
+@pytest.mark.parametrize("kind", [q.HOP_PACKED16, q.HOP_PACKED16_ACC16], ids=["packed16", "packed16_acc16"])
+@pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
+def test_mixed_precision_with_packed_hop(oracle_lib, sloppy, kind):
+    """The packed 16-bit hop inside the mixed solver: its Schur epilogues and fused
+    reductions drive the sloppy iteration, FP64 reliable updates keep the true residual."""
+    L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 4, 0.124, 1e-10
+    q.check(q.lib().qcuSetHopKernel(kind))
+    try:
+        gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 15, kind="smooth", t_boundary=-1.0,
+                                         opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy,
+                                               "reliable_delta": 0.003})
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
+    assert st == q.SUCCESS, q.last_error()
+    res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.all(true_rel <= tol)
+
+
 def test_invert_not_converged_status():
     L, nc, m = (4, 4, 4, 4), 3, 2
     gauge, b, x, st, stats = _invert(L, nc, m, 0.12, 1e-14, 16, max_iter=3)

@@ -85,3 +85,26 @@ def test_device_entry_points_validate_before_launch(qlib):
     assert rc == qlib.ERR_INVALID
     rc = lib.qcuMrhsNorm(None, None, 10, 65, qlib.DOUBLE, None)
     assert rc == qlib.ERR_INVALID
+
+
+def test_batch_rejects_bad_arguments_without_a_gpu(qlib):
+    lib = qlib.lib()
+    assert lib.qcuInvertBatch(None, 1, None, 0) == qlib.ERR_INVALID
+    arr = (qlib.QcuBatchSystem * 1)()
+    assert lib.qcuInvertBatch(arr, 0, None, 0) == qlib.ERR_INVALID
+    arr[0].lattice_size[:] = [4, 4, 4, 4]
+    arr[0].n_color, arr[0].m_rhs, arr[0].kappa, arr[0].tol = 3, 1, 0.1, 1e-10
+    assert lib.qcuInvertBatch(arr, 1, None, 0) == qlib.ERR_INVALID   # null gauge and fields
+    assert "null" in qlib.last_error()
+
+
+def test_precond_rejects_bad_arguments_without_a_gpu(qlib):
+    import ctypes as C
+    lib = qlib.lib()
+    h = C.c_void_p()
+    assert lib.qcuPrecondCreate(C.byref(h), qlib.lattice((7, 4, 4, 4)), 3, 4, 4, 8, 1.0) == qlib.ERR_INVALID
+    assert lib.qcuPrecondCreate(C.byref(h), qlib.lattice((8, 4, 4, 4)), 5, 4, 4, 8, 1.0) == qlib.ERR_UNSUPPORTED
+    assert lib.qcuPrecondCreate(C.byref(h), qlib.lattice((8, 4, 4, 4)), 3, 4, 0, 8, 1.0) == qlib.ERR_INVALID
+    assert lib.qcuPrecondCreate(C.byref(h), qlib.lattice((8, 4, 4, 4)), 3, 4, 4, 8, 0.5) == qlib.ERR_INVALID
+    assert not h.value
+    assert lib.qcuPrecondApply(None, None, None, qlib.DOUBLE, None) == qlib.ERR_INVALID
