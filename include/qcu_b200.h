@@ -235,12 +235,14 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
  *   TENSOR   FP16/BF16 storage on the tcgen05 tensor cores with TMEM accumulators and
  *            bulk-copy (TMA) staged neighbour spinors, for 2 <= n_color <= 4 and
  *            m_rhs <= 32 (else SIMT);
- *   PACKED16 FP16/BF16 storage, links staged once per site in shared memory, projection
- *            and link products in packed 16-bit complex arithmetic, the 8 hops summed
- *            in FP32; 2 <= n_color <= 4, m_rhs >= 2 (else SIMT);
+ *   PACKED16 FP16/BF16 storage, projection and link products in packed 16-bit complex
+ *            arithmetic, the 8 hops summed in FP32; 2 <= n_color <= 4, m_rhs >= 2
+ *            (else SIMT);
  *   PACKED16_ACC16  as PACKED16, with the 8 hops also summed in FP16 (FP16 storage
  *            only; the accumulation of the reference's half-precision path); less
  *            accurate, so AUTO never picks it;
+ *   PACKED16_STAGED as PACKED16, with each site's links staged once per block in shared
+ *            memory instead of read by each (site, RHS) thread;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else a static rule. */
 #define QCU_HOP_AUTO 0
@@ -249,6 +251,7 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
 #define QCU_HOP_SIMT_CS 3
 #define QCU_HOP_PACKED16 4
 #define QCU_HOP_PACKED16_ACC16 5
+#define QCU_HOP_PACKED16_STAGED 6
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

@@ -82,9 +82,9 @@ __device__ __forceinline__ int64_t h16_neighbour(const Geom& g, int64_t site, in
 
 // One hop of one (site, RHS): project the neighbour spinor, multiply by the staged link,
 // reconstruct into acc.  SG: sign s of gamma in this hop's projector (1 - s g or 1 + s g).
-template <int NC, typename S, bool ACC16, int MU, int SG, typename AccT>
+template <int NC, typename S, bool ACC16, int MU, int SG, typename AccT, typename LinkFn>
 __device__ __forceinline__ void h16_hop(AccT (&acc)[4][NC], const uint32_t* __restrict__ psi, int m,
-                                        const uint2* __restrict__ L) {
+                                        LinkFn link) {
     using P = Pk16<S>;
     using T2 = typename P::T2;
     uint32_t h0[NC], h1[NC];
@@ -121,40 +121,52 @@ __device__ __forceinline__ void h16_hop(AccT (&acc)[4][NC], const uint32_t* __re
         T2 w0 = word<T2>(0u), w1 = word<T2>(0u);
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-            const uint2 l = L[c * NC + k];
+            const uint2 l = link(c, k);
             w0 = P::fma(word<T2>(r0[k]), word<T2>(l.x), w0);
             w0 = P::fma(word<T2>(i0[k]), word<T2>(l.y), w0);
             w1 = P::fma(word<T2>(r1[k]), word<T2>(l.x), w1);
             w1 = P::fma(word<T2>(i1[k]), word<T2>(l.y), w1);
         }
         // reconstruction: acc0 += w0, acc1 += w1, acc2/acc3 from the projector
-        const uint32_t b0 = bits(w0), b1 = bits(w1);
-        uint32_t a2, a3;   // terms added to spins 2 and 3
-        if (MU == 0) {        // acc2 += -s i w1 ; acc3 += -s i w0
-            a2 = SG > 0 ? times_mi(b1) : times_i(b1);
-            a3 = SG > 0 ? times_mi(b0) : times_i(b0);
-        } else if (MU == 1) { // acc2 += s w1 ; acc3 += -s w0
-            a2 = SG > 0 ? b1 : b1 ^ 0x80008000u;
-            a3 = SG > 0 ? b0 ^ 0x80008000u : b0;
-        } else if (MU == 2) { // acc2 += -s i w0 ; acc3 += s i w1
-            a2 = SG > 0 ? times_mi(b0) : times_i(b0);
-            a3 = SG > 0 ? times_i(b1) : times_mi(b1);
-        } else {              // acc2 += s w0 ; acc3 += s w1
-            a2 = SG > 0 ? b0 : b0 ^ 0x80008000u;
-            a3 = SG > 0 ? b1 : b1 ^ 0x80008000u;
-        }
         if constexpr (ACC16) {
+            const uint32_t b0 = bits(w0), b1 = bits(w1);
+            uint32_t a2, a3;   // terms added to spins 2 and 3
+            if (MU == 0) {        // acc2 += -s i w1 ; acc3 += -s i w0
+                a2 = SG > 0 ? times_mi(b1) : times_i(b1);
+                a3 = SG > 0 ? times_mi(b0) : times_i(b0);
+            } else if (MU == 1) { // acc2 += s w1 ; acc3 += -s w0
+                a2 = SG > 0 ? b1 : b1 ^ 0x80008000u;
+                a3 = SG > 0 ? b0 ^ 0x80008000u : b0;
+            } else if (MU == 2) { // acc2 += -s i w0 ; acc3 += s i w1
+                a2 = SG > 0 ? times_mi(b0) : times_i(b0);
+                a3 = SG > 0 ? times_i(b1) : times_mi(b1);
+            } else {              // acc2 += s w0 ; acc3 += s w1
+                a2 = SG > 0 ? b0 : b0 ^ 0x80008000u;
+                a3 = SG > 0 ? b1 : b1 ^ 0x80008000u;
+            }
             acc[0][c] = P::add(acc[0][c], w0);
             acc[1][c] = P::add(acc[1][c], w1);
             acc[2][c] = P::add(acc[2][c], word<T2>(a2));
             acc[3][c] = P::add(acc[3][c], word<T2>(a3));
         } else {
+            // convert the two products once; the +-i and sign of spins 2, 3 are free in FP32
             const float2 f0 = P::f32(w0), f1 = P::f32(w1);
-            const float2 f2 = P::f32(word<T2>(a2)), f3 = P::f32(word<T2>(a3));
+            constexpr float sg = (float)SG;
             acc[0][c].x += f0.x; acc[0][c].y += f0.y;
             acc[1][c].x += f1.x; acc[1][c].y += f1.y;
-            acc[2][c].x += f2.x; acc[2][c].y += f2.y;
-            acc[3][c].x += f3.x; acc[3][c].y += f3.y;
+            if (MU == 0) {        // -i w = (w.im, -w.re)
+                acc[2][c].x += sg * f1.y; acc[2][c].y -= sg * f1.x;
+                acc[3][c].x += sg * f0.y; acc[3][c].y -= sg * f0.x;
+            } else if (MU == 1) {
+                acc[2][c].x += sg * f1.x; acc[2][c].y += sg * f1.y;
+                acc[3][c].x -= sg * f0.x; acc[3][c].y -= sg * f0.y;
+            } else if (MU == 2) {
+                acc[2][c].x += sg * f0.y; acc[2][c].y -= sg * f0.x;
+                acc[3][c].x -= sg * f1.y; acc[3][c].y += sg * f1.x;
+            } else {
+                acc[2][c].x += sg * f0.x; acc[2][c].y += sg * f0.y;
+                acc[3][c].x += sg * f1.x; acc[3][c].y += sg * f1.y;
+            }
         }
     }
 }
@@ -231,8 +243,9 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16_kernel(const HopParams p
             const uint2* L = sm.link + sl * H16Smem<NC>::kStride;
             const int* nbs = sm.nb[sl];
             const uint32_t* src = in + rhs;
-#define QCUB_H16_HOP(H, MU, SIGN) \
-    h16_hop<NC, S, ACC16, MU, SIGN>(acc, src + (int64_t)(nbs[H] & 0x7fffffff) * site_len, m, L + (H) * N2)
+#define QCUB_H16_HOP(H, MU, SIGN)                                                                     \
+    h16_hop<NC, S, ACC16, MU, SIGN>(acc, src + (int64_t)(nbs[H] & 0x7fffffff) * site_len, m,              \
+                                    [&](int c, int k) { return L[(H) * N2 + c * NC + k]; })
             QCUB_H16_HOP(0, 0, SF);
             QCUB_H16_HOP(1, 0, SB);
             QCUB_H16_HOP(2, 1, SF);
@@ -259,6 +272,158 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16_kernel(const HopParams p
         for (int k = 0; k < NV; ++k) rv[k] = red[k];
         grid_reduce<NV>(rv, m, p.red);
     }
+}
+
+// Variant without shared-memory staging: every (site, RHS) thread reads the links
+// itself (the m threads of a site read the same words) and forms (-W.im, W.re) in
+// registers; no block synchronisation, so the loads of different sites overlap freely.
+template <int NC, bool FWD>
+__device__ __forceinline__ void h16_load_link(uint32_t (&w)[NC * NC], const uint32_t* __restrict__ U, uint32_t flip) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+            w[c * NC + k] = FWD ? (__ldg(U + c * NC + k) ^ flip) : (__ldg(U + k * NC + c) ^ 0x80000000u ^ flip);
+}
+
+// MR > 0: the RHS count is the compile-time constant MR (p.m == MR), so every spinor
+// offset (s N + c) m is an immediate of its load; MR = 0: runtime m.
+template <int NC, typename S, bool DAG, int EPI, bool ACC16, int MR>
+__global__ void __launch_bounds__(kH16Threads, 3) hop16d_kernel(const HopParams p) {
+    using P = Pk16<S>;
+    using T2 = typename P::T2;
+    using AccT = typename std::conditional<ACC16, T2, float2>::type;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int N2 = NC * NC;
+    constexpr int SF = DAG ? 1 : -1;
+    constexpr int SB = DAG ? -1 : 1;
+    if (skip_launch(p.done, p.gate)) return;
+    const int m = MR > 0 ? MR : p.m;
+    const int rhs = threadIdx.x % m;
+    const int64_t vh = p.g.vh;
+    const int parity = p.parity;
+    const int64_t site_len = (int64_t)kNs * NC * m;
+    const uint32_t* __restrict__ in = static_cast<const uint32_t*>(p.in) + rhs;
+    const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
+    const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
+    const int lxh = p.g.lxh, Ly = p.g.L[1], Lz = p.g.L[2], Lt = p.g.L[3];
+    const int64_t sy = lxh, sz = (int64_t)lxh * Ly, st = sz * Lz;
+    const uint32_t* gf = gauge + (int64_t)parity * vh * N2;
+    const uint32_t* gb = gauge + (int64_t)(1 - parity) * vh * N2;
+    const int64_t gmu = 2 * vh * N2;
+    double2 red[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+    const int64_t site_stride = ((int64_t)gridDim.x * blockDim.x) / m;
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / m + threadIdx.x / m; site < vh; site += site_stride) {
+        const SiteXYZT c = site_coords(p.g, (uint32_t)site);
+        const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
+        AccT acc[4][NC];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) {
+                if constexpr (ACC16) acc[s][cc] = word<T2>(0u);
+                else acc[s][cc] = make_float2(0.f, 0.f);
+            }
+        uint32_t w[N2];
+        auto link = [&](int a, int b) { return make_uint2(w[a * NC + b], times_i(w[a * NC + b])); };
+        // x
+        {
+            const int64_t nf = site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh);
+            h16_load_link<NC, true>(w, gf + site * N2, 0u);
+            h16_hop<NC, S, ACC16, 0, SF>(acc, in + nf * site_len, m, link);
+            const int64_t nb = site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1));
+            h16_load_link<NC, false>(w, gb + nb * N2, 0u);
+            h16_hop<NC, S, ACC16, 0, SB>(acc, in + nb * site_len, m, link);
+        }
+        // y
+        {
+            const int64_t nf = site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy);
+            h16_load_link<NC, true>(w, gf + gmu + site * N2, 0u);
+            h16_hop<NC, S, ACC16, 1, SF>(acc, in + nf * site_len, m, link);
+            const int64_t nb = site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
+            h16_load_link<NC, false>(w, gb + gmu + nb * N2, 0u);
+            h16_hop<NC, S, ACC16, 1, SB>(acc, in + nb * site_len, m, link);
+        }
+        // z
+        {
+            const int64_t nf = site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz);
+            h16_load_link<NC, true>(w, gf + 2 * gmu + site * N2, 0u);
+            h16_hop<NC, S, ACC16, 2, SF>(acc, in + nf * site_len, m, link);
+            const int64_t nb = site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
+            h16_load_link<NC, false>(w, gb + 2 * gmu + nb * N2, 0u);
+            h16_hop<NC, S, ACC16, 2, SB>(acc, in + nb * site_len, m, link);
+        }
+        // t (the wrap sign is folded into the link)
+        {
+            const bool wf = (c.t + 1 == Lt);
+            const int64_t nf = site + (wf ? -(int64_t)(Lt - 1) * st : st);
+            h16_load_link<NC, true>(w, gf + 3 * gmu + site * N2, wf ? tflip : 0u);
+            h16_hop<NC, S, ACC16, 3, SF>(acc, in + nf * site_len, m, link);
+            const bool wb = (c.t == 0);
+            const int64_t nb = site + (wb ? (int64_t)(Lt - 1) * st : -st);
+            h16_load_link<NC, false>(w, gb + 3 * gmu + nb * N2, wb ? tflip : 0u);
+            h16_hop<NC, S, ACC16, 3, SB>(acc, in + nb * site_len, m, link);
+        }
+        float2 facc[4][NC];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) {
+                if constexpr (ACC16) facc[s][cc] = P::f32(acc[s][cc]);
+                else facc[s][cc] = acc[s][cc];
+            }
+        if constexpr (MR > 0) {
+            HopParams q = p;   // lets hop_store see the constant RHS count
+            q.m = MR;
+            hop_store<NC, S, EPI, NV>(facc, q, site * site_len + rhs, red);
+        } else {
+            hop_store<NC, S, EPI, NV>(facc, p, site * site_len + rhs, red);
+        }
+    }
+    if constexpr (NV > 0) {
+        double2 rv[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        grid_reduce<NV>(rv, m, p.red);
+    }
+}
+
+template <int NC, typename S, bool ACC16, int MR>
+int launch16d_m(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
+        return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
+    void (*k)(const HopParams) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop16d_kernel<NC, S, true, EPI_PLAIN, ACC16, MR> : hop16d_kernel<NC, S, false, EPI_PLAIN, ACC16, MR>; break;
+        case EPI_XPAY: k = dagger ? hop16d_kernel<NC, S, true, EPI_XPAY, ACC16, MR> : hop16d_kernel<NC, S, false, EPI_XPAY, ACC16, MR>; break;
+        case EPI_SCHUR_R0: k = hop16d_kernel<NC, S, false, EPI_SCHUR_R0, ACC16, MR>; break;
+        case EPI_SCHUR_TS: k = hop16d_kernel<NC, S, false, EPI_SCHUR_TS, ACC16, MR>; break;
+        case EPI_SCHUR: k = hop16d_kernel<NC, S, false, EPI_SCHUR, ACC16, MR>; break;
+        case EPI_RESID: k = hop16d_kernel<NC, S, false, EPI_RESID, ACC16, MR>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    const int block = (kH16Threads / p.m) * p.m;
+    int grid = resident_grid(k, block, p.g.vh * p.m);
+    if (grid > kScratchBlocks) grid = kScratchBlocks;
+    k<<<grid, block, 0, st>>>(p);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
+// RHS counts with a compile-time specialisation (SU(3) only; other shapes use runtime m)
+template <int NC, typename S, bool ACC16>
+int launch16d(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    if constexpr (NC == 3) {
+        switch (p.m) {
+            case 8: return launch16d_m<NC, S, ACC16, 8>(p, dagger, epi, st);
+            case 12: return launch16d_m<NC, S, ACC16, 12>(p, dagger, epi, st);
+            case 16: return launch16d_m<NC, S, ACC16, 16>(p, dagger, epi, st);
+            default: break;
+        }
+    }
+    return launch16d_m<NC, S, ACC16, 0>(p, dagger, epi, st);
 }
 
 template <int NC, typename S, bool ACC16>
@@ -293,22 +458,27 @@ bool hop16_supported(int nc, int m, int prec) {
            m <= kH16Threads;
 }
 
-// acc16: accumulate the 8 hops in the storage format (FP16 only)
-int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, cudaStream_t st) {
+// acc16: accumulate the 8 hops in the storage format (FP16 only); staged: read the links
+// through the shared-memory staging pass (else every thread reads its own)
+int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, bool staged,
+                 cudaStream_t st) {
     if (!hop16_supported(nc, p.m, prec)) return set_error(QCU_ERR_UNSUPPORTED, "packed 16-bit hop: n_color %d, m %d", nc, p.m);
     if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");
+    const bool a16 = acc16 && prec == QCU_PRECISION_HALF;
+#define QCUB_H16_NC(NCV, SV, A16) (staged ? launch16<NCV, SV, A16>(p, dagger, epi, st) : launch16d<NCV, SV, A16>(p, dagger, epi, st))
     if (prec == QCU_PRECISION_HALF) {
         switch (nc) {
-            case 2: return acc16 ? launch16<2, __half, true>(p, dagger, epi, st) : launch16<2, __half, false>(p, dagger, epi, st);
-            case 3: return acc16 ? launch16<3, __half, true>(p, dagger, epi, st) : launch16<3, __half, false>(p, dagger, epi, st);
-            default: return acc16 ? launch16<4, __half, true>(p, dagger, epi, st) : launch16<4, __half, false>(p, dagger, epi, st);
+            case 2: return a16 ? QCUB_H16_NC(2, __half, true) : QCUB_H16_NC(2, __half, false);
+            case 3: return a16 ? QCUB_H16_NC(3, __half, true) : QCUB_H16_NC(3, __half, false);
+            default: return a16 ? QCUB_H16_NC(4, __half, true) : QCUB_H16_NC(4, __half, false);
         }
     }
     switch (nc) {
-        case 2: return launch16<2, __nv_bfloat16, false>(p, dagger, epi, st);
-        case 3: return launch16<3, __nv_bfloat16, false>(p, dagger, epi, st);
-        default: return launch16<4, __nv_bfloat16, false>(p, dagger, epi, st);
+        case 2: return QCUB_H16_NC(2, __nv_bfloat16, false);
+        case 3: return QCUB_H16_NC(3, __nv_bfloat16, false);
+        default: return QCUB_H16_NC(4, __nv_bfloat16, false);
     }
+#undef QCUB_H16_NC
 }
 
 }  // namespace qcub

@@ -125,7 +125,8 @@ bool hop_tc_supported(int nc, int m, int prec);
 int auto_hop_kind(int nc, int m, int prec);
 int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 bool hop16_supported(int nc, int m, int prec);
-int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, cudaStream_t st);
+int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, bool staged,
+                 cudaStream_t st);
 
 // ---------------- hop dispatch ----------------
 template <typename S>
@@ -152,9 +153,10 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec) &&
         reinterpret_cast<uintptr_t>(p.in) % 16 == 0)
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
-    if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16) && hop16_supported(nc, p.m, prec))
-        return hop16_launch(p, nc, prec, dagger, epi, kind == QCU_HOP_PACKED16_ACC16 && prec == QCU_PRECISION_HALF,
-                            st);
+    if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16 || kind == QCU_HOP_PACKED16_STAGED) &&
+        hop16_supported(nc, p.m, prec))
+        return hop16_launch(p, nc, prec, dagger, epi, kind == QCU_HOP_PACKED16_ACC16,
+                            kind == QCU_HOP_PACKED16_STAGED, st);
     const bool cs = (kind == QCU_HOP_SIMT_CS) && nc * p.m <= kRedThreads;
     return dispatch_prec(prec, [&](auto tag) { return hop_nc<decltype(tag)>(p, nc, dagger, epi, st, cs); });
 }

@@ -97,8 +97,9 @@ def _acc16_factor(kind, prec):
     return 2.0 if (kind == q.HOP_PACKED16_ACC16 and prec == q.HALF) else 1.0
 
 
-LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16]
-LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16"]
+LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16,
+                q.HOP_PACKED16_STAGED]
+LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged"]
 
 
 @pytest.mark.parametrize("hop_kernel", LOWP_KERNELS, indirect=True, ids=LOWP_IDS)
@@ -120,8 +121,8 @@ def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
     assert q.lib().qcuGetKernelError(1) == 0
 
 
-@pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16], indirect=True,
-                         ids=["tcgen05", "packed16", "packed16_acc16"])
+@pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_STAGED],
+                         indirect=True, ids=["tcgen05", "packed16", "packed16_acc16", "packed16_staged"])
 @pytest.mark.parametrize("prec", [q.HALF, q.BF16])
 @pytest.mark.parametrize("L", [(2, 2, 2, 2), (6, 2, 4, 2), (4, 4, 4, 6), (8, 8, 8, 10)])
 def test_low_precision_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel):
