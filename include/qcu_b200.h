@@ -244,7 +244,8 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
  *   PACKED16_STAGED as PACKED16, with each site's links staged once per block in shared
  *            memory instead of read by each (site, RHS) thread;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
- *            (n_color, m_rhs, precision), else a static rule. */
+ *            (n_color, m_rhs, precision), else PACKED16 where it applies and SIMT
+ *            otherwise. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2

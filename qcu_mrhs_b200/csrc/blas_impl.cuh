@@ -27,6 +27,21 @@ __device__ __forceinline__ A2 from_d2(double2 v) {
     return mk2<A2>((decltype(A2::x))v.x, (decltype(A2::x))v.y);
 }
 
+// Per-thread partial sums of the solver's fused reductions: FP32 for 16-bit storage (the
+// inputs carry 1e-3 relative noise), FP64 otherwise; the sums across threads and blocks
+// are FP64.  The standalone dotc / norm kernels keep FP64 partials at every precision.
+template <typename S> struct RedAcc { using T = double; };
+template <> struct RedAcc<__half> { using T = float; };
+template <> struct RedAcc<__nv_bfloat16> { using T = float; };
+
+template <typename R, int NV>
+__device__ __forceinline__ void reduce_partials(const R (&v)[NV][2], int m, const RedArgs& ra) {
+    double2 d[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) d[k] = make_double2((double)v[k][0], (double)v[k][1]);
+    grid_reduce<NV>(d, m, ra);
+}
+
 #define QCUB_GRID_LOOP(gi, n)                                                                \
     for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < (n);            \
          gi += (int64_t)gridDim.x * blockDim.x)
@@ -35,25 +50,27 @@ template <typename S>
 __global__ void __launch_bounds__(kRedThreads) dotc_kernel(const typename St<S>::S2* __restrict__ a,
                                                            const typename St<S>::S2* __restrict__ b,
                                                            int64_t n, int m, RedArgs ra) {
-    double2 v[1] = {make_double2(0.0, 0.0)};
+    using R = double;   // the standalone reductions keep FP64 partial sums at every precision
+    R v[1][2] = {{0, 0}};
     QCUB_GRID_LOOP(gi, n) {
         const auto x = St<S>::ld(a[gi]);
         const auto y = St<S>::ld(b[gi]);
-        v[0].x += (double)x.x * y.x + (double)x.y * y.y;
-        v[0].y += (double)x.x * y.y - (double)x.y * y.x;
+        v[0][0] += (R)x.x * y.x + (R)x.y * y.y;
+        v[0][1] += (R)x.x * y.y - (R)x.y * y.x;
     }
-    grid_reduce<1>(v, m, ra);
+    reduce_partials<R, 1>(v, m, ra);
 }
 
 template <typename S>
 __global__ void __launch_bounds__(kRedThreads) norm2_kernel(const typename St<S>::S2* __restrict__ a,
                                                             int64_t n, int m, RedArgs ra) {
-    double2 v[1] = {make_double2(0.0, 0.0)};
+    using R = double;   // the standalone reductions keep FP64 partial sums at every precision
+    R v[1][2] = {{0, 0}};
     QCUB_GRID_LOOP(gi, n) {
         const auto x = St<S>::ld(a[gi]);
-        v[0].x += (double)x.x * x.x + (double)x.y * x.y;
+        v[0][0] += (R)x.x * x.x + (R)x.y * x.y;
     }
-    grid_reduce<1>(v, m, ra);
+    reduce_partials<R, 1>(v, m, ra);
 }
 
 template <typename S, int OP>
@@ -142,7 +159,8 @@ bicg_xr_kernel(typename St<SX>::S2* __restrict__ x, typename St<S>::S2* __restri
     const X2 al = from_d2<X2>(sc->alpha[j]);
     const X2 om = from_d2<X2>(sc->omega[j]);
     const A2 omA = from_d2<A2>(sc->omega[j]);
-    double2 v[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    using R = typename RedAcc<S>::T;
+    R v[2][2] = {{0, 0}, {0, 0}};
     QCUB_GRID_LOOP(gi, n) {
         const A2 pv = St<S>::ld(p[gi]);
         const A2 sv = St<S>::ld(s[gi]);
@@ -158,11 +176,11 @@ bicg_xr_kernel(typename St<SX>::S2* __restrict__ x, typename St<S>::S2* __restri
         r[gi] = rs;
         const A2 rv = St<S>::ld(rs);
         const A2 q = St<S>::ld(r0[gi]);
-        v[0].x += (double)rv.x * rv.x + (double)rv.y * rv.y;
-        v[1].x += (double)q.x * rv.x + (double)q.y * rv.y;
-        v[1].y += (double)q.x * rv.y - (double)q.y * rv.x;
+        v[0][0] += (R)rv.x * rv.x + (R)rv.y * rv.y;
+        v[1][0] += (R)q.x * rv.x + (R)q.y * rv.y;
+        v[1][1] += (R)q.x * rv.y - (R)q.y * rv.x;
     }
-    grid_reduce<2>(v, m, ra);
+    reduce_partials<R, 2>(v, m, ra);
 }
 
 // p = r + beta (p - omega v)

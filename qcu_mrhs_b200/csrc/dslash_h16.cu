@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16_kernel(const HopParams p
     const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
     const int sl = threadIdx.x / m;
     const int rhs = threadIdx.x - sl * m;
-    double2 red[NV > 0 ? NV : 1];
+    float2 red[NV > 0 ? NV : 1];   // per-thread partial sums (FP64 across threads and blocks)
 #pragma unroll
-    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_float2(0.f, 0.f);
 
     for (int64_t base = (int64_t)blockIdx.x * spb; base < vh; base += (int64_t)gridDim.x * spb) {
         __syncthreads();   // the previous pass has finished reading the staged links
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16_kernel(const HopParams p
     if constexpr (NV > 0) {
         double2 rv[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        for (int k = 0; k < NV; ++k) rv[k] = make_double2((double)red[k].x, (double)red[k].y);
         grid_reduce<NV>(rv, m, p.red);
     }
 }
@@ -289,7 +289,7 @@ __device__ __forceinline__ void h16_load_link(uint32_t (&w)[NC * NC], const uint
 // MR > 0: the RHS count is the compile-time constant MR (p.m == MR), so every spinor
 // offset (s N + c) m is an immediate of its load; MR = 0: runtime m.
 template <int NC, typename S, bool DAG, int EPI, bool ACC16, int MR>
-__global__ void __launch_bounds__(kH16Threads, 3) hop16d_kernel(const HopParams p) {
+__global__ void __launch_bounds__(kH16Threads, 4) hop16d_kernel(const HopParams p) {
     using P = Pk16<S>;
     using T2 = typename P::T2;
     using AccT = typename std::conditional<ACC16, T2, float2>::type;
@@ -311,11 +311,21 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16d_kernel(const HopParams 
     const uint32_t* gf = gauge + (int64_t)parity * vh * N2;
     const uint32_t* gb = gauge + (int64_t)(1 - parity) * vh * N2;
     const int64_t gmu = 2 * vh * N2;
-    double2 red[NV > 0 ? NV : 1];
+    float2 red[NV > 0 ? NV : 1];   // per-thread partial sums (FP64 across threads and blocks)
 #pragma unroll
-    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_float2(0.f, 0.f);
     const int64_t site_stride = ((int64_t)gridDim.x * blockDim.x) / m;
     for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / m + threadIdx.x / m; site < vh; site += site_stride) {
+        if constexpr (EPI != EPI_PLAIN) {
+            // the epilogue operands of this site (a contiguous site_len-word block) are
+            // fetched into L2 while the hops are computed: one 128-byte line per thread
+            const int64_t off = (int64_t)rhs * 32;   // words
+            if (off < site_len) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.x) + site * site_len + off));
+                if (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.r0) + site * site_len + off));
+            }
+        }
         const SiteXYZT c = site_coords(p.g, (uint32_t)site);
         const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
         AccT acc[4][NC];
@@ -385,7 +395,7 @@ __global__ void __launch_bounds__(kH16Threads, 3) hop16d_kernel(const HopParams 
     if constexpr (NV > 0) {
         double2 rv[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        for (int k = 0; k < NV; ++k) rv[k] = make_double2((double)red[k].x, (double)red[k].y);
         grid_reduce<NV>(rv, m, p.red);
     }
 }

@@ -198,7 +198,7 @@ __device__ __forceinline__ void hop_site(typename St<S>::A2 (&acc)[4][NC], const
 // `base` is the offset of (site, spin 0, colour 0, RHS) in the gathered layout.
 template <int NC, typename S, int EPI, int NV>
 __device__ __forceinline__ void hop_store(const typename St<S>::A2 (&acc)[4][NC], const HopParams& p,
-                                          int64_t base, double2 (&red)[NV > 0 ? NV : 1]) {
+                                          int64_t base, typename St<S>::A2 (&red)[NV > 0 ? NV : 1]) {
     using S2 = typename St<S>::S2;
     using A = typename St<S>::A;
     using A2 = typename St<S>::A2;
@@ -229,17 +229,19 @@ __device__ __forceinline__ void hop_store(const typename St<S>::A2 (&acc)[4][NC]
                 const S2 rs = St<S>::cv(res);
                 out[o] = rs;
                 if (NV > 0) {
+                    // per-thread partial sums in the arithmetic type (FP64 for FP64 storage,
+                    // FP32 otherwise); the sums across threads and blocks are FP64
                     const A2 rr = St<S>::ld(rs);
                     if (EPI == EPI_RESID) {
-                        red[0].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                        red[0].x += rr.x * rr.x + rr.y * rr.y;
                     } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
                         const A2 q = St<S>::ld(r0[o]);
-                        red[0].x += (double)q.x * rr.x + (double)q.y * rr.y;
-                        red[0].y += (double)q.x * rr.y - (double)q.y * rr.x;
+                        red[0].x += q.x * rr.x + q.y * rr.y;
+                        red[0].y += q.x * rr.y - q.y * rr.x;
                     } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
-                        red[0].x += (double)rr.x * xx.x + (double)rr.y * xx.y;
-                        red[0].y += (double)rr.x * xx.y - (double)rr.y * xx.x;
-                        red[NV - 1].x += (double)rr.x * rr.x + (double)rr.y * rr.y;
+                        red[0].x += rr.x * xx.x + rr.y * xx.y;
+                        red[0].y += rr.x * xx.y - rr.y * xx.x;
+                        red[NV - 1].x += rr.x * rr.x + rr.y * rr.y;
                     }
                 }
             }
@@ -266,9 +268,9 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
     const int64_t total = p.g.vh * m;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t site_len = (int64_t)kNs * NC * m;
-    double2 red[NV > 0 ? NV : 1];
+    A2 red[NV > 0 ? NV : 1];
 #pragma unroll
-    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = mk2<A2>(0, 0);
 
     // block size and grid stride are multiples of m: the thread keeps RHS tid % m and
     // walks sites without dividing
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
     if constexpr (NV > 0) {
         double2 rv[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) rv[k] = red[k];
+        for (int k = 0; k < NV; ++k) rv[k] = make_double2((double)red[k].x, (double)red[k].y);
         grid_reduce<NV>(rv, m, p.red);
     }
 }

@@ -4,30 +4,13 @@
 // Same operator and layouts as dslash_impl.cuh (reference
 // include/kernel/su_n_m_rhs_dslash.cuh:92-105, complex_matmul.cuh:16-600).
 //
-// Formulation.  For a site x and one of its 8 hops h, the contribution to out(x) is
-//   out_h[s][c][r] = sum_c' W_h[c][c'] * P_h[s][c'][r],   P_h = (1 -+ s g_mu) psi(x +- mu)
-// (W_h = U_mu(x) forward, U_mu(x-mu)^dagger backward).  The 4-spinor projection P_h is
-// formed row by row; (s, r) rows share the link, so this is a real GEMM with
-//   M = rows (site, s, r),  K = (c', re/im),  N = (c, re/im)
-// and B = the real embedding of W_h^T.  Two sites share one M = 128 tile when
-// 4m <= 64 and 2N <= 8: their K and N ranges are disjoint blocks (B block-diagonal),
-// so one instruction computes both sites' hop.  All 8 hops accumulate into the same
-// tensor-memory tile.
-//
-// Data path per tile (one CTA = 128 threads = 128 tile rows, thread i <-> TMEM lane i):
-//   A  (128 x 16 bf16/f16) in TMEM: each thread projects its row in packed 16-bit
-//      arithmetic and writes it with tcgen05.st (8 x 32-bit columns);
-//   B  (16 x 16) in shared memory, K-major, no swizzle: written from the links;
-//   D  (128 x 16 fp32) in TMEM, tcgen05.mma kind::f16 issued by one thread, completion
-//      signalled through tcgen05.commit to an mbarrier;
-//   per tile: every thread issues the loads of all 8 hops first (they overlap the
-//      previous tile's MMAs), then waits for those MMAs, runs the previous tile's
-//      epilogue, writes the 8 A rows and 8 B tiles, one barrier, and one thread issues
-//      the 8 MMAs back to back and one commit;
-//   epilogue: tcgen05.ld of the thread's row, conversion, store (and the fused
-//      Schur/xpay epilogues and per-RHS reductions of the SIMT kernel).
-// Every wait on an mbarrier is bounded; on timeout the kernel records an error code
-// and finishes (results are then invalid, never a hang).
+// The kernel (hop_mma_kernel, below) turns the 8 hops of a site into one real GEMM with
+// K = 8 hops x 2N: A rows are the projected neighbour spinors (spin, RHS), B the real
+// embedding of the 8 link matrices.  A and B are written to shared memory by the CTA's
+// threads; tcgen05.mma kind::f16 (M = 128, N = 16, K = 16, issued by one thread) sums
+// into tensor memory; completion is signalled through tcgen05.commit to an mbarrier.
+// Every wait on an mbarrier is bounded; on timeout the kernel records an error code and
+// finishes (results are then invalid, never a hang).
 #include "dslash.h"
 #include "dslash_impl.cuh"
 #include "workspace.h"
@@ -37,10 +20,6 @@ namespace qcub {
 int* device_error_flag();   // runtime.cu: per-device flag, nonzero after a timed-out wait
 
 namespace tc {
-
-constexpr int kThreads = 128;
-constexpr int kTmemCols = 128;         // D: 16 columns, A: 8 hops x 8 columns (80 used)
-constexpr int kColD = 0, kColA = 16;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -77,13 +56,6 @@ __device__ __forceinline__ void fence_after_sync() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-        : "memory");
-}
-
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
     asm volatile(
@@ -113,16 +85,6 @@ __host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt) {
     return (1u << 4) | (fmt << 7) | (fmt << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                      smem_u32(bar))
@@ -148,16 +110,6 @@ __device__ __forceinline__ uint32_t as_u32(T2 v) {
 template <typename T2>
 __device__ __forceinline__ T2 from_u32(uint32_t u) {
     return *reinterpret_cast<T2*>(&u);
-}
-__device__ __forceinline__ uint32_t swap_halves(uint32_t u) { return __byte_perm(u, 0, 0x1032); }
-
-// Partner spin p(s) and sign of gamma_mu[s][p(s)] (DeGrand-Rossi, reference qcu_gamma.cuh);
-// gamma_1 and gamma_3 entries are imaginary.
-__device__ __forceinline__ int partner(int mu, int s) { return mu < 2 ? 3 - s : (s ^ 2); }
-__device__ __forceinline__ float gsign(int mu, int s) {
-    // mu=0: +i,+i,-i,-i ; mu=1: -1,+1,+1,-1 ; mu=2: +i,-i,-i,+i ; mu=3: +1,+1,+1,+1
-    // nibble mu of 0x069C has bit s set where the entry is negative
-    return ((0x069Cu >> (4 * mu + s)) & 1u) ? -1.f : 1.f;
 }
 
 struct Tile {
@@ -206,117 +158,158 @@ __device__ __forceinline__ SiteCoord coords(const Geom& geo, int64_t site, int p
     return c;
 }
 
-// B tile: 16 (n) x 16 (k) 16-bit values, K-major core matrices: (n/8, k/8) at
-// (n/8)*256 + (k/8)*128 bytes, row n%8 at +16*(n%8), element k%8 at +2*(k%8).
-__device__ __forceinline__ int b_word(int n, int k) {   // 32-bit word index of (n, k..k+1), k even
-    return ((n >> 3) * 256 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2) >> 2;
-}
+// =====================================================================================
+// One GEMM per pair of sites (hop_mma_kernel) -- the kernel behind QCU_HOP_TENSOR.
+//
+// For a site x the 8 hops form one real matrix product:
+//   out[s'][c][r] = sum_{h, c', ri} A[(s', r)][(h, c', ri)] * B[(h, c', ri)][(c, ro)]
+//   A row (s', r): the projected neighbour spinor of every hop,
+//       R_h[s'][c'][r] = psi_{x+h}[s'][c'][r] + coef_h(s') psi_{x+h}[p_h(s')][c'][r];
+//   B: the real embedding of W_h^T (W_h = U_mu(x) forward, U_mu(x - mu)^dag backward;
+//       column (c, re) holds (Re W, -Im W) over (c', re/im), column (c, im) (Im W, Re W)).
+// K = 8 hops x 2N = 16N: N MMAs of K = 16 per tile.  Two sites share an M = 128 tile
+// (rows 0..4m-1 site a, 4m..8m-1 site b) and B = [B_a | B_b] (8 columns each), so site a's
+// rows read columns 0..7 of D and site b's rows columns 8..15 (no block-diagonal zeros).
+// A and B live in shared memory (K-major, no swizzle); D (128 lanes x 16 FP32 columns per
+// tile) in tensor memory.  A CTA of 128 threads processes T tiles per round: the threads
+// write A and B, one thread issues the T x N MMAs and a commit, every thread waits on the
+// commit's mbarrier (bounded), then reads its own TMEM lane (= its A row) and writes it.
+// =====================================================================================
+constexpr int kMmaThreads = 128;
+constexpr int kMmaMaxTiles = 5;
+constexpr int kMmaTmemCols = 128;   // T x 16 <= 80 columns used
 
-// Projected row value of one hop: row_s = psi_s + coef * psi_p(s) in packed 16-bit math.
-template <typename P2>
-__device__ __forceinline__ uint32_t project(uint32_t a, uint32_t b, bool imag, P2 cvec) {
-    if (imag) b = swap_halves(b);
-    return as_u32(__hfma2(from_u32<P2>(b), cvec, from_u32<P2>(a)));
-}
+// Partner spin p(s) and sign of gamma_mu[s][p(s)] in the DeGrand-Rossi basis (reference
+// include/kernel/qcu_gamma.cuh): mu=0: +i,+i,-i,-i ; mu=1: -1,+1,+1,-1 ; mu=2: +i,-i,-i,+i ;
+// mu=3: +1,+1,+1,+1 (gamma_1 and gamma_3 entries are imaginary); nibble mu of 0x069C has
+// bit s set where the entry is negative.
+__host__ __device__ constexpr int gsign_c(int mu, int s) { return ((0x069C >> (4 * mu + s)) & 1) ? -1 : 1; }
+__host__ __device__ constexpr int partner_c(int mu, int s) { return mu < 2 ? 3 - s : (s ^ 2); }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-// bulk global -> shared copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(a), "r"(b),
-                 "r"(c), "r"(d)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr)
-                 : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-#pragma unroll
-    for (int i = 8; i < 16; ++i) v[i] = 0.f;
-}
-
-constexpr int kStages = 3;
-constexpr int kCTA = 160;       // 4 consumer warps (TMEM lanes 0..127) + 1 producer warp
-
-// Shared-memory plan (32-bit words): kStages x { spinors [spt][8 hops][site_len],
-// links [spt][8 hops][N*N] }, then 8 B tiles of 128 words.
-struct TcPlan {
-    int spt, rows_block, site_len, stage_words, link_off;
+struct MmaPlan {
+    int S;          // sites per tile (2 when 8m <= 128)
+    int T;          // tiles per round
+    int K;          // 16 N
+    int a_bytes;    // 128 x K 16-bit values
+    int b_bytes;    // 16 x K 16-bit values
 };
-__host__ __device__ inline TcPlan tc_plan(int nc, int m) {
-    TcPlan q;
-    q.spt = (4 * m <= 64 && 2 * nc <= 8) ? 2 : 1;
-    q.rows_block = q.spt == 2 ? 64 : 128;
-    q.site_len = 4 * nc * m;
-    q.link_off = q.spt * 8 * q.site_len;
-    q.stage_words = q.link_off + q.spt * 8 * nc * nc;
-    q.stage_words = (q.stage_words + 31) & ~31;   // keep every stage 128-byte aligned
+__host__ __device__ inline MmaPlan mma_plan(int nc, int m) {
+    MmaPlan q;
+    q.S = (8 * m <= 128) ? 2 : 1;
+    q.K = 16 * nc;
+    const int per_tile = q.S * m;
+    q.T = kMmaThreads / per_tile;
+    if (q.T > kMmaMaxTiles) q.T = kMmaMaxTiles;
+    if (q.T < 1) q.T = 1;
+    q.a_bytes = 128 * q.K * 2;
+    q.b_bytes = 16 * q.K * 2;
     return q;
 }
-inline size_t tc_smem_bytes(int nc, int m) {
-    const TcPlan q = tc_plan(nc, m);
-    return (size_t)(kStages * q.stage_words + 8 * 128) * 4;
+inline size_t mma_smem_bytes(int nc, int m) {
+    const MmaPlan q = mma_plan(nc, m);
+    return (size_t)q.T * (q.a_bytes + q.b_bytes);
+}
+
+// byte offset of (row n, k) in a K-major, no-swizzle operand with R row groups:
+// core matrix (n / 8, k / 8) at ((k / 8) * R + n / 8) * 128, row n % 8 at +16, k % 8 at +2
+__device__ __forceinline__ uint32_t kmajor_off(int n, int k, int row_groups) {
+    return (uint32_t)((((k >> 3) * row_groups + (n >> 3)) << 7) + ((n & 7) << 4) + ((k & 7) << 1));
+}
+
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// packed-word helpers (re low half, im high half)
+__device__ __forceinline__ uint32_t w_times_i(uint32_t u) { return __byte_perm(u, 0, 0x1032) ^ 0x00008000u; }
+__device__ __forceinline__ uint32_t w_times_mi(uint32_t u) { return __byte_perm(u, 0, 0x1032) ^ 0x80000000u; }
+
+template <typename S>
+__device__ __forceinline__ uint32_t w_add(uint32_t a, uint32_t b) {
+    return as_u32(__hadd2(from_u32<typename Pk<S>::T2>(a), from_u32<typename Pk<S>::T2>(b)));
+}
+
+// a + cs * (imag ? i b : b), cs = +-1 known at compile time
+template <typename S, int CS, bool IMAG>
+__device__ __forceinline__ uint32_t w_project(uint32_t a, uint32_t b) {
+    uint32_t t;
+    if (IMAG) t = CS > 0 ? w_times_i(b) : w_times_mi(b);
+    else t = CS > 0 ? b : (b ^ 0x80008000u);
+    return w_add<S>(a, t);
+}
+
+template <int NC, typename S, bool DAG, int H>
+__device__ __forceinline__ void mma_rows_hop(uint32_t (&rw)[4][4 * NC], const uint32_t* __restrict__ src, int m) {
+    constexpr int MU = H >> 1;
+    constexpr bool FWD = (H & 1) == 0;
+    constexpr bool IMAG = (MU == 0 || MU == 2);
+    constexpr int SG = FWD ? (DAG ? 1 : -1) : (DAG ? -1 : 1);   // 1 + SG gamma_mu
+    uint32_t v[4][NC];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) v[s][c] = __ldg(src + (s * NC + c) * m);
+    constexpr int hl = H & 3;   // position of the hop in its group of 4
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        rw[0][hl * NC + c] = w_project<S, SG * gsign_c(MU, 0), IMAG>(v[0][c], v[partner_c(MU, 0)][c]);
+        rw[1][hl * NC + c] = w_project<S, SG * gsign_c(MU, 1), IMAG>(v[1][c], v[partner_c(MU, 1)][c]);
+        rw[2][hl * NC + c] = w_project<S, SG * gsign_c(MU, 2), IMAG>(v[2][c], v[partner_c(MU, 2)][c]);
+        rw[3][hl * NC + c] = w_project<S, SG * gsign_c(MU, 3), IMAG>(v[3][c], v[partner_c(MU, 3)][c]);
+    }
 }
 
 template <int NC, typename S, bool DAG, int EPI>
-__global__ void __launch_bounds__(kCTA, 3) hop_tc_kernel(const HopParams p, int* err) {
+__global__ void __launch_bounds__(kMmaThreads) hop_mma_kernel(const HopParams p, int* err) {
     using S2 = typename St<S>::S2;
     using A2 = typename St<S>::A2;
-    using P2 = typename Pk<S>::T2;
     constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
     constexpr int N2 = NC * NC;
-    extern __shared__ __align__(128) uint32_t smem[];
-    __shared__ __align__(8) uint64_t sFull[kStages];
-    __shared__ __align__(8) uint64_t sEmpty[kStages];
+    extern __shared__ __align__(128) uint8_t smem8[];
     __shared__ __align__(8) uint64_t sMma;
     __shared__ uint32_t sTmem;
-    __shared__ double2 sRed[NV > 0 ? NV * kMaxRhs : 1];
-    __shared__ double2 sRow[NV > 0 ? NV * 128 : 1];
+    __shared__ int sNb[kMmaMaxTiles][2][8];
+    __shared__ int sAbort;
 
     if (skip_launch(p.done, p.gate)) return;
     const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
+    const int warp = tid >> 5;
     const int m = p.m;
-    const TcPlan plan = tc_plan(NC, m);
-    const int spt = plan.spt;
-    const int site_len = plan.site_len;
+    const MmaPlan plan = mma_plan(NC, m);
+    const int S_ = plan.S, T = plan.T;
+    const int rows_used = S_ * 4 * m;
     const int64_t vh = p.g.vh;
-    const int64_t ntiles = (vh + spt - 1) / spt;
     const int parity = p.parity;
-    uint32_t* sB = smem + kStages * plan.stage_words;
+    const int64_t site_len = (int64_t)kNs * NC * m;
+    const int64_t per_round = (int64_t)T * S_;
+    const int64_t nrounds = (vh + per_round - 1) / per_round;
+    const uint32_t* __restrict__ in = static_cast<const uint32_t*>(p.in);
+    const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
+    const int64_t gmu = 2 * vh * N2;
+    const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
+    uint8_t* sA = smem8;                                   // T tiles of a_bytes
+    uint8_t* sB = smem8 + (size_t)T * plan.a_bytes;        // T tiles of b_bytes
 
-    // ---- one-time set-up ----
+    // ---- set-up: zero A and B once (unused rows / columns stay zero), TMEM, mbarrier ----
+    {
+        uint4* z = reinterpret_cast<uint4*>(smem8);
+        const int n16 = T * (plan.a_bytes + plan.b_bytes) / 16;
+        for (int i = tid; i < n16; i += kMmaThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(&sFull[s], 1 + spt * 8);   // producer's expect_tx + one per staged link
-            mbar_init(&sEmpty[s], 128);          // every consumer thread releases the stage
-        }
         mbar_init(&sMma, 1);
+        sAbort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 8 * 128; i += kCTA) sB[i] = 0u;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sTmem)),
-                     "r"(kTmemCols)
+                     "r"(kMmaTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -324,106 +317,145 @@ __global__ void __launch_bounds__(kCTA, 3) hop_tc_kernel(const HopParams p, int*
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = sTmem;
+    const uint32_t idesc = instr_desc(Pk<S>::fmt);   // M = 128, N = 16, K-major A and B
+
+    // producer role of this thread: (tile, slot, RHS)
+    const int per_tile = S_ * m;
+    const int pt = tid / per_tile;
+    const int pslot = (tid % per_tile) / m;
+    const int prr = tid % m;
+    const bool producer = pt < T;
+    // epilogue role: TMEM lane = A row = tid
+    const bool row_used = tid < rows_used;
+    const int eslot = row_used ? tid / (4 * m) : 0;
+    const int ewithin = tid - eslot * 4 * m;
+    const int esp = row_used ? ewithin / m : 0;
+    const int err_ = ewithin - esp * m;   // RHS of this row
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+
+    A2 red[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = mk2<A2>(0, 0);
+    uint32_t phase = 0;
     bool timed_out = false;
 
-    if (warp == 4) {
-        // ================= producer warp: stage neighbour spinors and links =================
-        const S2* __restrict__ in = static_cast<const S2*>(p.in);
-        const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
-        const int64_t gmu = 2 * vh * N2;
-        const uint32_t site_bytes = (uint32_t)site_len * 4u;
-        int64_t it = 0;
-        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-            const int stage = (int)(it % kStages);
-            if (it >= kStages && !timed_out) {
-                if (!mbar_wait(&sEmpty[stage], (uint32_t)((it / kStages) - 1) & 1u)) timed_out = true;
-            }
-            uint32_t* st = smem + stage * plan.stage_words;
-            const int64_t site0 = tile * spt;
-            const int nvalid = (int)((vh - site0) < spt ? (vh - site0) : spt);
-            if (lane == 0) mbar_arrive_tx(&sFull[stage], (uint32_t)nvalid * 8u * site_bytes);
-            __syncwarp();
-            if (lane < spt * 8) {
-                const int sl = lane >> 3, h = lane & 7, mu = h >> 1;
-                const bool fwd = (h & 1) == 0;
-                const int64_t site = site0 + sl;
-                if (sl < nvalid) {
-                    const SiteCoord c = coords(p.g, site, parity);
-                    bool wrap;
-                    const Tile tg{p.g.lxh, p.g.L[1], p.g.L[2], p.g.L[3], vh};
-                    const int64_t nb = neighbour(tg, site, c.xh, c.y, c.z, c.t, c.xodd, mu, fwd, &wrap);
-                    bulk_g2s(st + (sl * 8 + h) * site_len, in + nb * site_len, site_bytes, &sFull[stage]);
-                    const uint32_t* U = fwd ? gauge + (int64_t)parity * vh * N2 + mu * gmu + site * N2
-                                            : gauge + (int64_t)(1 - parity) * vh * N2 + mu * gmu + nb * N2;
-                    const uint32_t flip = (wrap && p.t_sign < 0) ? 0x80008000u : 0u;
-                    uint32_t* dl = st + plan.link_off + (sl * 8 + h) * N2;
+    for (int64_t round = blockIdx.x; round < nrounds; round += gridDim.x) {
+        const int64_t base = round * per_round;
+        // ---- neighbours of this thread's site (producers) ----
+        int64_t psite = base + (int64_t)pt * S_ + pslot;
+        const bool pvalid = producer && psite < vh;
+        int64_t nbs[8];
+        uint32_t wrapf = 0;
+        if (pvalid) {
+            const SiteCoord c = coords(p.g, psite, parity);
+            const Tile tg{p.g.lxh, p.g.L[1], p.g.L[2], p.g.L[3], vh};
 #pragma unroll
-                    for (int e = 0; e < N2; ++e) dl[e] = __ldg(U + e) ^ flip;
+            for (int h = 0; h < 8; ++h) {
+                bool wrap;
+                nbs[h] = neighbour(tg, psite, c.xh, c.y, c.z, c.t, c.xodd, h >> 1, (h & 1) == 0, &wrap);
+                if (wrap) wrapf |= 1u << h;
+            }
+            if (prr == 0)
+#pragma unroll
+                for (int h = 0; h < 8; ++h) sNb[pt][pslot][h] = (int)nbs[h] | (((wrapf >> h) & 1u) ? (int)0x80000000u : 0);
+        }
+        __syncthreads();   // sNb visible; the previous round's epilogue has finished with TMEM
+        // ---- B: real embedding of the links, T x S x 8 x N x N items of two words ----
+        {
+            const int nitems = T * S_ * 8 * N2;
+            for (int it = tid; it < nitems; it += kMmaThreads) {
+                int q = it;
+                const int cc = q % NC; q /= NC;       // c'
+                const int c = q % NC; q /= NC;        // c
+                const int h = q % 8; q /= 8;
+                const int sl = q % S_;
+                const int t = q / S_;
+                const int64_t site = base + (int64_t)t * S_ + sl;
+                if (site >= vh) continue;
+                const int mu = h >> 1;
+                const int nbw = sNb[t][sl][h];
+                uint32_t w;
+                if ((h & 1) == 0) {
+                    w = __ldg(gauge + (int64_t)parity * vh * N2 + mu * gmu + site * N2 + c * NC + cc);
+                } else {
+                    const int64_t nb = nbw & 0x7fffffff;
+                    w = __ldg(gauge + (int64_t)(1 - parity) * vh * N2 + mu * gmu + nb * N2 + cc * NC + c) ^ 0x80000000u;
                 }
-                mbar_arrive(&sFull[stage]);   // release: the link words above are visible to consumers
+                if (nbw < 0) w ^= tflip;
+                uint8_t* bt = sB + (size_t)t * plan.b_bytes;
+                const int k = h * 2 * NC + 2 * cc;
+                const int n = sl * 8 + 2 * c;
+                *reinterpret_cast<uint32_t*>(bt + kmajor_off(n, k, 2)) = w ^ 0x80000000u;        // (Re W, -Im W)
+                *reinterpret_cast<uint32_t*>(bt + kmajor_off(n + 1, k, 2)) = __byte_perm(w, 0, 0x1032);   // (Im W, Re W)
             }
         }
-        // drain: every bulk copy this CTA issued has landed before the CTA can exit (bounded;
-        // in a healthy run the consumers already waited on all of these phases)
-        if (lane == 0) {
-            for (int64_t k = (it > kStages ? it - kStages : 0); k < it; ++k)
-                if (!mbar_wait(&sFull[(int)(k % kStages)], (uint32_t)(k / kStages) & 1u)) timed_out = true;
-        }
-    } else {
-        // ================= consumer warps: A rows (TMEM), B tiles, MMA, epilogue =================
-        const int rows_block = plan.rows_block;
-        const int sl = tid / rows_block;
-        const int within = tid - sl * rows_block;
-        const bool row_used = sl < spt && within < 4 * m;
-        const int sp = row_used ? within / m : 0;
-        const int rr = row_used ? within - sp * m : 0;
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-        const uint32_t idesc = instr_desc(Pk<S>::fmt);
-        const int kb = spt == 2 ? 8 : 16;
-        // projection coefficient per hop: 1 + sigma gamma_mu, sigma = -s forward, +s backward
-        P2 cvec[8];
+        // ---- A: 4 rows (s' = 0..3) of this thread's (site, RHS), hops in two groups of 4 ----
+        if (pvalid) {
+            uint8_t* at = sA + (size_t)pt * plan.a_bytes;
+            const uint32_t* src = in + prr;
 #pragma unroll
-        for (int h = 0; h < 8; ++h) {
-            const int mu = h >> 1;
-            const float cs = ((h & 1) == 0 ? (DAG ? 1.f : -1.f) : (DAG ? -1.f : 1.f)) * gsign(mu, sp);
-            cvec[h] = (mu == 0 || mu == 2) ? Pk<S>::sgn(-cs, cs) : Pk<S>::sgn(cs, cs);
-        }
-        const int pp_lo = partner(0, sp), pp_hi = partner(2, sp);   // partner for mu < 2, mu >= 2
-        // B work item: (site block, c_out, ri_out, c_in)
-        const bool b_worker = tid < spt * NC * 2 * NC;
-        int b_sl = 0, b_cout = 0, b_riout = 0, b_cin = 0;
-        if (b_worker) {
-            int q = tid;
-            b_cin = q % NC; q /= NC;
-            b_riout = q % 2; q /= 2;
-            b_cout = q % NC;
-            b_sl = q / NC;
-        }
-        const int b_word_idx = b_worker ? b_word(b_sl * kb + 2 * b_cout + b_riout, b_sl * kb + 2 * b_cin) : 0;
-
-        // zero this row's A columns once (the other site's block and padding stay zero)
+            for (int g = 0; g < 2; ++g) {
+                uint32_t rw[4][4 * NC];
+                if (g == 0) {
+                    mma_rows_hop<NC, S, DAG, 0>(rw, src + nbs[0] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 1>(rw, src + nbs[1] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 2>(rw, src + nbs[2] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 3>(rw, src + nbs[3] * site_len, m);
+                } else {
+                    mma_rows_hop<NC, S, DAG, 4>(rw, src + nbs[4] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 5>(rw, src + nbs[5] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 6>(rw, src + nbs[6] * site_len, m);
+                    mma_rows_hop<NC, S, DAG, 7>(rw, src + nbs[7] * site_len, m);
+                }
+                // 4 N words = N chunks of 16 bytes per row; the group starts at K = 32 N g
 #pragma unroll
-        for (int h = 0; h < 8; ++h) tmem_st4(tmem + lane_base + kColA + 8 * h, 0u, 0u, 0u, 0u),
-                                    tmem_st4(tmem + lane_base + kColA + 8 * h + 4, 0u, 0u, 0u, 0u);
-
-        double2 red[NV > 0 ? NV : 1];
+                for (int s = 0; s < 4; ++s) {
+                    const int n = pslot * 4 * m + s * m + prr;
 #pragma unroll
-        for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[k] = make_double2(0.0, 0.0);
-
-        auto epilogue = [&](int64_t site, bool valid) {
+                    for (int ch = 0; ch < NC; ++ch) {
+                        const int k = g * 8 * NC + ch * 8;
+                        *reinterpret_cast<uint4*>(at + kmajor_off(n, k, 16)) =
+                            make_uint4(rw[s][4 * ch], rw[s][4 * ch + 1], rw[s][4 * ch + 2], rw[s][4 * ch + 3]);
+                    }
+                }
+            }
+        }
+        // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        fence_before_sync();
+        __syncthreads();
+        if (tid == 0 && !timed_out) {
+            fence_after_sync();
+            for (int t = 0; t < T; ++t) {
+#pragma unroll
+                for (int ks = 0; ks < NC; ++ks) {
+                    const uint64_t ad = smem_desc(sA + (size_t)t * plan.a_bytes + ks * 2 * 16 * 128, 16 * 128, 128);
+                    const uint64_t bd = smem_desc(sB + (size_t)t * plan.b_bytes + ks * 2 * 2 * 128, 2 * 128, 128);
+                    mma_ss(tmem + (uint32_t)(16 * t), ad, bd, idesc, ks > 0 ? 1u : 0u);
+                }
+            }
+            mma_commit(&sMma);
+        }
+        // ---- wait for the MMAs (bounded), then every thread reads its TMEM lane ----
+        if (!timed_out && !mbar_wait(&sMma, phase)) {
+            timed_out = true;
+            sAbort = 1;
+        }
+        phase ^= 1u;
+        fence_after_sync();
+        for (int t = 0; t < T; ++t) {
             float d[16];
-            if (spt == 2) tmem_ld8(tmem + lane_base + kColD + 8 * sl, d);
-            else tmem_ld16(tmem + lane_base + kColD, d);
-            fence_before_sync();
-            if (!valid) return;
+            tmem_ld16(tmem + lane_base + (uint32_t)(16 * t), d);
+            const int64_t site = base + (int64_t)t * S_ + eslot;
+            if (!row_used || site >= vh || timed_out) continue;
             S2* __restrict__ out = static_cast<S2*>(p.out);
             const S2* __restrict__ xv = static_cast<const S2*>(p.x);
             const S2* __restrict__ r0v = static_cast<const S2*>(p.r0);
-            const int64_t base = site * site_len + rr;
+            const int64_t obase = site * site_len + err_;
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const int64_t o = base + (int64_t)(sp * NC + c) * m;
-                const A2 v = mk2<A2>(d[2 * c], d[2 * c + 1]);
+                const int64_t o = obase + (int64_t)(esp * NC + c) * m;
+                const A2 v = mk2<A2>(d[eslot * 8 + 2 * c], d[eslot * 8 + 2 * c + 1]);
                 if (EPI == EPI_PLAIN) {
                     out[o] = St<S>::cv(v);
                 } else {
@@ -443,200 +475,103 @@ __global__ void __launch_bounds__(kCTA, 3) hop_tc_kernel(const HopParams p, int*
                     if (NV > 0) {
                         const A2 q = St<S>::ld(rs);
                         if (EPI == EPI_RESID) {
-                            red[0].x += (double)q.x * q.x + (double)q.y * q.y;
+                            red[0].x += q.x * q.x + q.y * q.y;
                         } else if (EPI == EPI_SCHUR_R0) {
                             const A2 z = St<S>::ld(r0v[o]);
-                            red[0].x += (double)z.x * q.x + (double)z.y * q.y;
-                            red[0].y += (double)z.x * q.y - (double)z.y * q.x;
+                            red[0].x += z.x * q.x + z.y * q.y;
+                            red[0].y += z.x * q.y - z.y * q.x;
                         } else if (EPI == EPI_SCHUR_TS) {
-                            red[0].x += (double)q.x * xx.x + (double)q.y * xx.y;
-                            red[0].y += (double)q.x * xx.y - (double)q.y * xx.x;
-                            red[NV - 1].x += (double)q.x * q.x + (double)q.y * q.y;
+                            red[0].x += q.x * xx.x + q.y * xx.y;
+                            red[0].y += q.x * xx.y - q.y * xx.x;
+                            red[NV - 1].x += q.x * q.x + q.y * q.y;
                         }
                     }
                 }
             }
-        };
-
-        uint32_t mma_phase = 0;
-        bool pending = false;
-        int64_t prev_site = 0;
-        bool prev_valid = false;
-        int64_t it = 0;
-        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-            const int stage = (int)(it % kStages);
-            if (!timed_out && !mbar_wait(&sFull[stage], (uint32_t)(it / kStages) & 1u)) timed_out = true;
-            const uint32_t* st = smem + stage * plan.stage_words;
-            const int64_t my_site = tile * spt + sl;
-            const bool row_valid = row_used && my_site < vh;
-            // ---- operands of the 8 hops from the staged tile ----
-            uint32_t va[8][NC], vb[8][NC], wl[8];
-            const uint32_t* rowp = st + sl * 8 * site_len + rr;
-#pragma unroll
-            for (int h = 0; h < 8; ++h) {
-                const int pp = (h >> 1) < 2 ? pp_lo : pp_hi;
-#pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    va[h][c] = row_valid ? rowp[h * site_len + (sp * NC + c) * m] : 0u;
-                    vb[h][c] = row_valid ? rowp[h * site_len + (pp * NC + c) * m] : 0u;
-                }
-                if (b_worker) {
-                    const bool fwd = (h & 1) == 0;
-                    const uint32_t uu =
-                        st[plan.link_off + (b_sl * 8 + h) * N2 + (fwd ? b_cout * NC + b_cin : b_cin * NC + b_cout)];
-                    // forward W = U: (W_re,-W_im) | (W_im,W_re); backward W = U^dag: (U_re,U_im) | (-U_im,U_re)
-                    wl[h] = fwd ? (b_riout == 0 ? (uu ^ 0x80000000u) : swap_halves(uu))
-                                : (b_riout == 0 ? uu : (swap_halves(uu) ^ 0x00008000u));
-                }
-            }
-            mbar_arrive(&sEmpty[stage]);   // stage consumed (values are in registers)
-            // ---- previous tile: MMAs done -> epilogue; frees D, A and B ----
-            if (pending) {
-                if (tid == 0 && !timed_out && !mbar_wait(&sMma, mma_phase)) timed_out = true;
-                mma_phase ^= 1u;
-                consumer_sync();
-                fence_after_sync();
-                epilogue(prev_site, prev_valid);
-            }
-            // ---- A rows and B tiles ----
-#pragma unroll
-            for (int h = 0; h < 8; ++h) {
-                const bool imag = ((h >> 1) == 0 || (h >> 1) == 2);
-                uint32_t r[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c) r[c] = project(va[h][c], vb[h][c], imag, cvec[h]);
-                if (spt == 2) {
-                    tmem_st4(tmem + lane_base + kColA + 8 * h + 4 * sl, r[0], NC > 1 ? r[NC > 1 ? 1 : 0] : 0u,
-                             NC > 2 ? r[NC > 2 ? 2 : 0] : 0u, NC > 3 ? r[NC > 3 ? 3 : 0] : 0u);
-                } else {
-                    uint32_t av[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) av[j] = j < NC ? r[j < NC ? j : 0] : 0u;
-                    tmem_st8(tmem + lane_base + kColA + 8 * h, av);
-                }
-                if (b_worker) sB[h * 128 + b_word_idx] = wl[h];
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-            fence_before_sync();
-            consumer_sync();
-            if (tid == 0) {
-                fence_after_sync();
-#pragma unroll
-                for (int h = 0; h < 8; ++h)
-                    mma_ts(tmem + kColD, tmem + kColA + 8 * h, smem_desc(sB + h * 128, 128, 256), idesc,
-                           h > 0 ? 1u : 0u);
-                mma_commit(&sMma);
-            }
-            pending = true;
-            prev_site = my_site;
-            prev_valid = row_valid;
         }
-        if (pending) {   // always wait (bounded) for the last MMAs before TMEM is freed
-            if (tid == 0 && !mbar_wait(&sMma, mma_phase)) timed_out = true;
-            consumer_sync();
-            fence_after_sync();
-            epilogue(prev_site, prev_valid);
-        }
-        if constexpr (NV > 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) sRow[k * 128 + tid] = row_used ? red[k] : make_double2(0.0, 0.0);
-        }
+        fence_before_sync();
+        __syncthreads();
+        if (sAbort) break;   // uniform: every thread read sAbort after the barrier
     }
 
-    // all MMAs have completed and every stage has been consumed; free TMEM
+    // every MMA of this CTA completed (or its wait gave up); free TMEM
     fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         fence_after_sync();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMmaTmemCols)
                      : "memory");
     }
     if (timed_out && err != nullptr) atomicExch(err, 1);
-
     if constexpr (NV > 0) {
-        // per-RHS block sums in a fixed order: rows of the same RHS, in row order
-        const int rows_block = plan.rows_block;
-        for (int idx = tid; idx < NV * m; idx += kCTA) {
-            const int k = idx / m, j = idx - k * m;
-            double2 s = make_double2(0.0, 0.0);
-            for (int i = 0; i < 128; ++i) {
-                const int bsl = i / rows_block, w = i - bsl * rows_block;
-                if (bsl < spt && w < 4 * m && w % m == j) {
-                    s.x += sRow[k * 128 + i].x;
-                    s.y += sRow[k * 128 + i].y;
-                }
-            }
-            sRed[idx] = s;
-        }
-        __syncthreads();
-        publish_and_finish<NV>(sRed, m, p.red);
+        double2 rv[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rv[k] = make_double2((double)red[k].x, (double)red[k].y);
+        grid_reduce<NV>(rv, m, p.red);
     }
 }
 
 template <int NC, typename S>
-int launch_tc(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
-    void (*k)(const HopParams, int*) = nullptr;
-    switch (epi) {
-        case EPI_PLAIN: k = dagger ? hop_tc_kernel<NC, S, true, EPI_PLAIN> : hop_tc_kernel<NC, S, false, EPI_PLAIN>; break;
-        case EPI_XPAY: k = dagger ? hop_tc_kernel<NC, S, true, EPI_XPAY> : hop_tc_kernel<NC, S, false, EPI_XPAY>; break;
-        case EPI_SCHUR_R0: k = hop_tc_kernel<NC, S, false, EPI_SCHUR_R0>; break;
-        case EPI_SCHUR_TS: k = hop_tc_kernel<NC, S, false, EPI_SCHUR_TS>; break;
-        case EPI_SCHUR: k = hop_tc_kernel<NC, S, false, EPI_SCHUR>; break;
-        case EPI_RESID: k = hop_tc_kernel<NC, S, false, EPI_RESID>; break;
-        default: return set_error(QCU_ERR_INVALID, "unknown hop epilogue %d", epi);
-    }
+int launch_mma(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
         return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
-    const size_t smem = tc_smem_bytes(NC, p.m);
+    void (*k)(const HopParams, int*) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop_mma_kernel<NC, S, true, EPI_PLAIN> : hop_mma_kernel<NC, S, false, EPI_PLAIN>; break;
+        case EPI_XPAY: k = dagger ? hop_mma_kernel<NC, S, true, EPI_XPAY> : hop_mma_kernel<NC, S, false, EPI_XPAY>; break;
+        case EPI_SCHUR_R0: k = hop_mma_kernel<NC, S, false, EPI_SCHUR_R0>; break;
+        case EPI_SCHUR_TS: k = hop_mma_kernel<NC, S, false, EPI_SCHUR_TS>; break;
+        case EPI_SCHUR: k = hop_mma_kernel<NC, S, false, EPI_SCHUR>; break;
+        case EPI_RESID: k = hop_mma_kernel<NC, S, false, EPI_RESID>; break;
+        default: return set_error(QCU_ERR_INVALID, "unknown hop epilogue %d", epi);
+    }
+    const size_t smem = mma_smem_bytes(NC, p.m);
     static bool attr_set[2][6] = {};
     const int di = dagger ? 1 : 0;
     if (!attr_set[di][epi]) {
         QCUB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr_set[di][epi] = true;
     }
-    const TcPlan plan = tc_plan(NC, p.m);
-    const int64_t ntiles = (p.g.vh + plan.spt - 1) / plan.spt;
-    int per_sm = blocks_per_sm(reinterpret_cast<const void*>(k), kCTA, smem);
-    if (per_sm <= 1) {   // occupancy query unavailable: estimate from the register count
-        cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, k) == cudaSuccess && fa.numRegs > 0)
-            per_sm = 65536 / (((fa.numRegs + 7) / 8 * 8) * kCTA);
+    const MmaPlan plan = mma_plan(NC, p.m);
+    const int64_t per_round = (int64_t)plan.T * plan.S;
+    const int64_t nrounds = (p.g.vh + per_round - 1) / per_round;
+    int per_sm = blocks_per_sm(reinterpret_cast<const void*>(k), kMmaThreads, smem);
+    if (per_sm <= 1) {   // occupancy query unavailable: estimate from shared memory
+        per_sm = (int)((220 * 1024) / (smem + 4096));
         cudaGetLastError();
     }
-    const int tmem_cap = 512 / kTmemCols;   // CTAs per SM that can hold their TMEM at once
+    const int tmem_cap = 512 / kMmaTmemCols;
     if (per_sm > tmem_cap) per_sm = tmem_cap;
     if (per_sm < 1) per_sm = 1;
     const int64_t cap = (int64_t)per_sm * sm_count();
-    int grid = (int)(ntiles < cap ? ntiles : cap);
+    int grid = (int)(nrounds < cap ? nrounds : cap);
     if (grid > kScratchBlocks) grid = kScratchBlocks;
     if (grid < 1) grid = 1;
-    k<<<grid, kCTA, smem, st>>>(p, device_error_flag());
+    k<<<grid, kMmaThreads, smem, st>>>(p, device_error_flag());
     QCUB_CHECK_LAUNCH();
     return QCU_SUCCESS;
 }
 
 }  // namespace tc
 
-// Tensor-core hop for FP16/BF16 storage: n_color 2..4 and 4*m <= 128, input 16-byte aligned.
+// Tensor-core hop for FP16/BF16 storage: n_color 2..4 and 4*m <= 128.
 // Returns QCU_ERR_UNSUPPORTED for shapes it does not cover.
 bool hop_tc_supported(int nc, int m, int prec) {
     if (prec != QCU_PRECISION_HALF && prec != QCU_PRECISION_BF16) return false;
-    if (nc < 2 || nc > 4) return false;   // operands of 8 hops are held in registers
+    if (nc < 2 || nc > 4) return false;   // K = 16 N, one 16-byte chunk per hop group and colour
     return 4 * m <= 128;
 }
 
 int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
-    if (reinterpret_cast<uintptr_t>(p.in) % 16 != 0)
-        return set_error(QCU_ERR_UNSUPPORTED, "tensor-core hop: input spinor not 16-byte aligned");
     if (!hop_tc_supported(nc, p.m, prec))
         return set_error(QCU_ERR_UNSUPPORTED, "tensor-core hop: n_color=%d m=%d precision=%d", nc, p.m, prec);
+    if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");
     auto go = [&](auto tag) -> int {
         using S = decltype(tag);
         switch (nc) {
-            case 2: return tc::launch_tc<2, S>(p, dagger, epi, st);
-            case 3: return tc::launch_tc<3, S>(p, dagger, epi, st);
-            default: return tc::launch_tc<4, S>(p, dagger, epi, st);
+            case 2: return tc::launch_mma<2, S>(p, dagger, epi, st);
+            case 3: return tc::launch_mma<3, S>(p, dagger, epi, st);
+            default: return tc::launch_mma<4, S>(p, dagger, epi, st);
         }
     };
     if (prec == QCU_PRECISION_HALF) return go(__half{});

@@ -120,8 +120,8 @@ void set_hop_kind(int k) { g_hop_kind = k; }
 bool hop_tc_supported(int nc, int m, int prec);
 
 // Kernel used when the selection is AUTO: the tuned choice for (n_color, m, precision)
-// if one was recorded (qcuTuneHop / the tuning cache), else a static rule: colour-split
-// SIMT for N >= 5 (fewer registers per thread), per-(site, RHS) SIMT otherwise.
+// if one was recorded (qcuTuneHop / the tuning cache), else a static rule: the packed
+// 16-bit kernel for FP16/BF16 storage where it applies, per-(site, RHS) SIMT otherwise.
 int auto_hop_kind(int nc, int m, int prec);
 int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 bool hop16_supported(int nc, int m, int prec);

@@ -59,7 +59,9 @@ int auto_hop_kind(int nc, int m, int prec) {
         auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
         if (it != g_tuned.end()) return it->second;
     }
-    if (nc >= 5) return nc * m <= kRedThreads ? QCU_HOP_SIMT_CS : QCU_HOP_SIMT;
+    // measured on B200 (16^4, N = 3..8, m = 8..32): packed 16-bit arithmetic wins for
+    // FP16/BF16 storage wherever it applies, the per-(site, RHS) SIMT kernel everywhere else
+    if (hop16_supported(nc, m, prec)) return QCU_HOP_PACKED16;
     return QCU_HOP_SIMT;
 }
 
