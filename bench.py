@@ -117,14 +117,32 @@ def dist_setup():
     return world, rank, local
 
 
+def reduce_max(v, world, device):
+    """Max of a per-rank value over all ranks of the initialised process group (any
+    backend: NCCL on the GPUs, gloo in the CPU tests)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seeds(rank):
+    """Seeds of one replica: every rank solves its own seeded system (weak scaling)."""
+    return SEED_GAUGE + rank, SEED_SRC + rank
+
+
 def make_fields(rank):
     """The benchmark's fields, generated on the host with torch's seeded CPU generator
     (identical for both legs): gauge [4][2][Vh][3][3] and sources [12][2][Vh][4][3]."""
     import torch
     from qcu_mrhs_b200 import fields as F
     torch.set_num_threads(os.cpu_count() or 1)
-    gauge = F.gauge_field_torch(L, NC, SEED_GAUGE + rank, kind="smooth", eps=EPS, device="cpu")
-    src = F.gaussian_fermions_torch(L, NC, M, SEED_SRC + rank, device="cpu")
+    sg, ss = replica_seeds(rank)
+    gauge = F.gauge_field_torch(L, NC, sg, kind="smooth", eps=EPS, device="cpu")
+    src = F.gaussian_fermions_torch(L, NC, M, ss, device="cpu")
     return gauge, src
 
 
@@ -229,7 +247,7 @@ def main():
         k = lib.qcuTuneHop(q.lattice(L), NC, M, prec, None)
         if k < 0:
             raise RuntimeError(f"autotuner: {q.last_error()}")
-        tuned[name] = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16"}.get(k, str(k))
+        tuned[name] = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs"}.get(k, str(k))
     torch.cuda.synchronize()
 
     def solve(srcs, outs, max_iter=MAX_ITER):
@@ -247,11 +265,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, world, "cuda")
 
     # ---- mixed precision (the product path: FP16 storage) ----
     set_opts(q.SOLVER_MIXED, q.HALF)

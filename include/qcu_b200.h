@@ -243,6 +243,8 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
  *            accurate, so AUTO never picks it;
  *   PACKED16_STAGED as PACKED16, with each site's links staged once per block in shared
  *            memory instead of read by each (site, RHS) thread;
+ *   PACKED16_PAIRS  as PACKED16 with two RHS per thread (8-byte neighbour loads, links
+ *            shared by the pair), SU(3) with m = 8, 12 or 16 (else PACKED16);
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else PACKED16 where it applies and SIMT
  *            otherwise. */
@@ -253,6 +255,7 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
 #define QCU_HOP_PACKED16 4
 #define QCU_HOP_PACKED16_ACC16 5
 #define QCU_HOP_PACKED16_STAGED 6
+#define QCU_HOP_PACKED16_PAIRS 7
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

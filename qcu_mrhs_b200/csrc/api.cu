@@ -611,7 +611,7 @@ int qcuGaugeFromEO(void* lex, const void* eo, const int L[4], int n_color, int p
 
 int qcuSetHopKernel(int kind) {
     clear_error();
-    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_STAGED)
+    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_PAIRS)
         return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
     set_hop_kind(kind);
     return QCU_SUCCESS;

@@ -422,6 +422,269 @@ int launch16d_m(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     return QCU_SUCCESS;
 }
 
+// ---- two RHS per thread (compile-time even m) ----
+// Thread per (half-site, RHS pair j): RHS 2j and 2j+1 sit in one 8-byte word pair of every
+// (spin, colour) row, so each neighbour value is one 8-byte load; the links, their
+// (-W.im, W.re) partners and the neighbour arithmetic serve both RHS.
+template <int NC, typename S, int MU, int SG, typename LinkFn>
+__device__ __forceinline__ void h16_hop2(float2 (&acc)[2][4][NC], const uint2* __restrict__ psi, int m2,
+                                         LinkFn link) {
+    using P = Pk16<S>;
+    using T2 = typename P::T2;
+    uint32_t h0[2][NC], h1[2][NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const uint2 q0 = __ldg(psi + (0 * NC + c) * m2);
+        const uint2 q1 = __ldg(psi + (1 * NC + c) * m2);
+        const uint2 q2 = __ldg(psi + (2 * NC + c) * m2);
+        const uint2 q3 = __ldg(psi + (3 * NC + c) * m2);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t p0 = r ? q0.y : q0.x, p1 = r ? q1.y : q1.x;
+            const uint32_t p2 = r ? q2.y : q2.x, p3 = r ? q3.y : q3.x;
+            if (MU == 0) {
+                h0[r][c] = bits(P::add(word<T2>(p0), word<T2>(SG > 0 ? times_i(p3) : times_mi(p3))));
+                h1[r][c] = bits(P::add(word<T2>(p1), word<T2>(SG > 0 ? times_i(p2) : times_mi(p2))));
+            } else if (MU == 1) {
+                h0[r][c] = bits(SG > 0 ? P::sub(word<T2>(p0), word<T2>(p3)) : P::add(word<T2>(p0), word<T2>(p3)));
+                h1[r][c] = bits(SG > 0 ? P::add(word<T2>(p1), word<T2>(p2)) : P::sub(word<T2>(p1), word<T2>(p2)));
+            } else if (MU == 2) {
+                h0[r][c] = bits(P::add(word<T2>(p0), word<T2>(SG > 0 ? times_i(p2) : times_mi(p2))));
+                h1[r][c] = bits(P::add(word<T2>(p1), word<T2>(SG > 0 ? times_mi(p3) : times_i(p3))));
+            } else {
+                h0[r][c] = bits(SG > 0 ? P::add(word<T2>(p0), word<T2>(p2)) : P::sub(word<T2>(p0), word<T2>(p2)));
+                h1[r][c] = bits(SG > 0 ? P::add(word<T2>(p1), word<T2>(p3)) : P::sub(word<T2>(p1), word<T2>(p3)));
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        T2 w0[2] = {word<T2>(0u), word<T2>(0u)}, w1[2] = {word<T2>(0u), word<T2>(0u)};
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const uint2 l = link(c, k);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                w0[r] = P::fma(word<T2>(bcast_re(h0[r][k])), word<T2>(l.x), w0[r]);
+                w0[r] = P::fma(word<T2>(bcast_im(h0[r][k])), word<T2>(l.y), w0[r]);
+                w1[r] = P::fma(word<T2>(bcast_re(h1[r][k])), word<T2>(l.x), w1[r]);
+                w1[r] = P::fma(word<T2>(bcast_im(h1[r][k])), word<T2>(l.y), w1[r]);
+            }
+        }
+        constexpr float sg = (float)SG;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const float2 f0 = P::f32(w0[r]), f1 = P::f32(w1[r]);
+            float2 (&a)[4][NC] = acc[r];
+            a[0][c].x += f0.x; a[0][c].y += f0.y;
+            a[1][c].x += f1.x; a[1][c].y += f1.y;
+            if (MU == 0) {
+                a[2][c].x += sg * f1.y; a[2][c].y -= sg * f1.x;
+                a[3][c].x += sg * f0.y; a[3][c].y -= sg * f0.x;
+            } else if (MU == 1) {
+                a[2][c].x += sg * f1.x; a[2][c].y += sg * f1.y;
+                a[3][c].x -= sg * f0.x; a[3][c].y -= sg * f0.y;
+            } else if (MU == 2) {
+                a[2][c].x += sg * f0.y; a[2][c].y -= sg * f0.x;
+                a[3][c].x -= sg * f1.y; a[3][c].y += sg * f1.x;
+            } else {
+                a[2][c].x += sg * f0.x; a[2][c].y += sg * f0.y;
+                a[3][c].x += sg * f1.x; a[3][c].y += sg * f1.y;
+            }
+        }
+    }
+}
+
+// Block and grid reduction when thread t holds the partial sums of RHS 2 (t % (m/2)) and
+// 2 (t % (m/2)) + 1: fixed summation order, then the common last-block finisher.
+template <int NV>
+__device__ inline void grid_reduce_pairs(const float2 (&v)[2][NV > 0 ? NV : 1], int m, const RedArgs& ra) {
+    __shared__ double2 sh[NV][2][kH16Threads];
+    __shared__ double2 bsum[NV * kMaxRhs];
+    const int tid = threadIdx.x, nb = blockDim.x, half = m >> 1;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) sh[k][q][tid] = make_double2((double)v[q][k].x, (double)v[q][k].y);
+    __syncthreads();
+    for (int idx = tid; idx < NV * m; idx += nb) {
+        const int k = idx / m, rhs = idx - k * m;
+        const int j = rhs >> 1, q = rhs & 1;
+        double2 s = make_double2(0.0, 0.0);
+        for (int t = j; t < nb; t += half) {
+            s.x += sh[k][q][t].x;
+            s.y += sh[k][q][t].y;
+        }
+        bsum[idx] = s;
+    }
+    __syncthreads();
+    publish_and_finish<NV>(bsum, m, ra);
+}
+
+template <int NC, typename S, bool DAG, int EPI, int MR>
+__global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams p) {
+    using P = Pk16<S>;
+    using S2 = typename St<S>::S2;
+    using A2 = typename St<S>::A2;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int N2 = NC * NC;
+    constexpr int SF = DAG ? 1 : -1;
+    constexpr int SB = DAG ? -1 : 1;
+    constexpr int M2 = MR / 2;
+    static_assert(MR % 2 == 0, "two RHS per thread need an even RHS count");
+    if (skip_launch(p.done, p.gate)) return;
+    const int j = threadIdx.x % M2;                // RHS pair
+    const int64_t vh = p.g.vh;
+    const int parity = p.parity;
+    constexpr int64_t site_len = (int64_t)kNs * NC * MR;   // words per site
+    const uint2* __restrict__ in2 = reinterpret_cast<const uint2*>(p.in) + j;
+    const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
+    const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
+    const int lxh = p.g.lxh, Ly = p.g.L[1], Lz = p.g.L[2], Lt = p.g.L[3];
+    const int64_t sy = lxh, sz = (int64_t)lxh * Ly, st = sz * Lz;
+    const uint32_t* gf = gauge + (int64_t)parity * vh * N2;
+    const uint32_t* gb = gauge + (int64_t)(1 - parity) * vh * N2;
+    const int64_t gmu = 2 * vh * N2;
+    float2 red[2][NV > 0 ? NV : 1];
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[q][k] = make_float2(0.f, 0.f);
+    const int64_t site_stride = ((int64_t)gridDim.x * blockDim.x) / M2;
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / M2 + threadIdx.x / M2; site < vh; site += site_stride) {
+        if constexpr (EPI != EPI_PLAIN) {
+            const int64_t off = (int64_t)j * 32;
+            if (off < site_len) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.x) + site * site_len + off));
+                if (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.r0) + site * site_len + off));
+            }
+        }
+        const SiteXYZT c = site_coords(p.g, (uint32_t)site);
+        const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
+        float2 acc[2][4][NC];
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) acc[r][s][cc] = make_float2(0.f, 0.f);
+        uint32_t w[N2];
+        auto link = [&](int a, int b) { return make_uint2(w[a * NC + b], times_i(w[a * NC + b])); };
+        constexpr int64_t sl2 = site_len / 2;   // uint2 per site
+        {
+            const int64_t nf = site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh);
+            h16_load_link<NC, true>(w, gf + site * N2, 0u);
+            h16_hop2<NC, S, 0, SF>(acc, in2 + nf * sl2, M2, link);
+            const int64_t nb = site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1));
+            h16_load_link<NC, false>(w, gb + nb * N2, 0u);
+            h16_hop2<NC, S, 0, SB>(acc, in2 + nb * sl2, M2, link);
+        }
+        {
+            const int64_t nf = site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy);
+            h16_load_link<NC, true>(w, gf + gmu + site * N2, 0u);
+            h16_hop2<NC, S, 1, SF>(acc, in2 + nf * sl2, M2, link);
+            const int64_t nb = site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
+            h16_load_link<NC, false>(w, gb + gmu + nb * N2, 0u);
+            h16_hop2<NC, S, 1, SB>(acc, in2 + nb * sl2, M2, link);
+        }
+        {
+            const int64_t nf = site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz);
+            h16_load_link<NC, true>(w, gf + 2 * gmu + site * N2, 0u);
+            h16_hop2<NC, S, 2, SF>(acc, in2 + nf * sl2, M2, link);
+            const int64_t nb = site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
+            h16_load_link<NC, false>(w, gb + 2 * gmu + nb * N2, 0u);
+            h16_hop2<NC, S, 2, SB>(acc, in2 + nb * sl2, M2, link);
+        }
+        {
+            const bool wf = (c.t + 1 == Lt);
+            const int64_t nf = site + (wf ? -(int64_t)(Lt - 1) * st : st);
+            h16_load_link<NC, true>(w, gf + 3 * gmu + site * N2, wf ? tflip : 0u);
+            h16_hop2<NC, S, 3, SF>(acc, in2 + nf * sl2, M2, link);
+            const bool wb = (c.t == 0);
+            const int64_t nb = site + (wb ? (int64_t)(Lt - 1) * st : -st);
+            h16_load_link<NC, false>(w, gb + 3 * gmu + nb * N2, wb ? tflip : 0u);
+            h16_hop2<NC, S, 3, SB>(acc, in2 + nb * sl2, M2, link);
+        }
+        // epilogue: the two RHS of every (spin, colour) row as one 8-byte word pair
+        uint2* __restrict__ out2 = reinterpret_cast<uint2*>(p.out);
+        const uint2* __restrict__ x2 = reinterpret_cast<const uint2*>(p.x);
+        const uint2* __restrict__ r02 = reinterpret_cast<const uint2*>(p.r0);
+        const int64_t base2 = site * sl2 + j;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) {
+                const int64_t o = base2 + (int64_t)(s * NC + cc) * M2;
+                if (EPI == EPI_PLAIN) {
+                    const S2 a0 = St<S>::cv(acc[0][s][cc]), a1 = St<S>::cv(acc[1][s][cc]);
+                    out2[o] = make_uint2(bits(a0), bits(a1));
+                } else {
+                    const uint2 xw = x2[o];
+                    uint2 yw = make_uint2(0u, 0u);
+                    if (EPI == EPI_RESID || EPI == EPI_SCHUR_R0) yw = r02[o];
+                    uint32_t res_bits[2];
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        const A2 v = acc[r][s][cc];
+                        const A2 xx = St<S>::ld(word<S2>(r ? xw.y : xw.x));
+                        const float a = (float)p.a;
+                        A2 res;
+                        if (EPI == EPI_XPAY) {
+                            res = mk2<A2>(xx.x + a * v.x, xx.y + a * v.y);
+                        } else if (EPI == EPI_RESID) {
+                            const A2 yy = St<S>::ld(word<S2>(r ? yw.y : yw.x));
+                            res = mk2<A2>(yy.x - xx.x + a * v.x, yy.y - xx.y + a * v.y);
+                        } else {
+                            res = mk2<A2>(xx.x - a * v.x, xx.y - a * v.y);
+                        }
+                        const S2 rs = St<S>::cv(res);
+                        res_bits[r] = bits(rs);
+                        if (NV > 0) {
+                            const A2 rr = St<S>::ld(rs);
+                            if (EPI == EPI_RESID) {
+                                red[r][0].x += rr.x * rr.x + rr.y * rr.y;
+                            } else if (EPI == EPI_SCHUR_R0) {
+                                const A2 q = St<S>::ld(word<S2>(r ? yw.y : yw.x));
+                                red[r][0].x += q.x * rr.x + q.y * rr.y;
+                                red[r][0].y += q.x * rr.y - q.y * rr.x;
+                            } else if (EPI == EPI_SCHUR_TS) {
+                                red[r][0].x += rr.x * xx.x + rr.y * xx.y;
+                                red[r][0].y += rr.x * xx.y - rr.y * xx.x;
+                                red[r][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                            }
+                        }
+                    }
+                    out2[o] = make_uint2(res_bits[0], res_bits[1]);
+                }
+            }
+    }
+    if constexpr (NV > 0) grid_reduce_pairs<NV>(red, MR, p.red);
+}
+
+template <int NC, typename S, int MR>
+int launch16p(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
+        return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
+    void (*k)(const HopParams) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop16p_kernel<NC, S, true, EPI_PLAIN, MR> : hop16p_kernel<NC, S, false, EPI_PLAIN, MR>; break;
+        case EPI_XPAY: k = dagger ? hop16p_kernel<NC, S, true, EPI_XPAY, MR> : hop16p_kernel<NC, S, false, EPI_XPAY, MR>; break;
+        case EPI_SCHUR_R0: k = hop16p_kernel<NC, S, false, EPI_SCHUR_R0, MR>; break;
+        case EPI_SCHUR_TS: k = hop16p_kernel<NC, S, false, EPI_SCHUR_TS, MR>; break;
+        case EPI_SCHUR: k = hop16p_kernel<NC, S, false, EPI_SCHUR, MR>; break;
+        case EPI_RESID: k = hop16p_kernel<NC, S, false, EPI_RESID, MR>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    constexpr int M2 = MR / 2;
+    const int block = (kH16Threads / M2) * M2;
+    int grid = resident_grid(k, block, p.g.vh * M2);
+    if (grid > kScratchBlocks) grid = kScratchBlocks;
+    k<<<grid, block, 0, st>>>(p);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
 // RHS counts with a compile-time specialisation (SU(3) only; other shapes use runtime m)
 template <int NC, typename S, bool ACC16>
 int launch16d(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
@@ -466,6 +729,27 @@ int launch16(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
 bool hop16_supported(int nc, int m, int prec) {
     return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc >= 2 && nc <= 4 && m >= 2 &&
            m <= kH16Threads;
+}
+
+// SU(3) shapes with a two-RHS-per-thread specialisation
+bool hop16_pairs_supported(int nc, int m, int prec) {
+    return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc == 3 && (m == 8 || m == 12 || m == 16);
+}
+
+int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
+    if (!hop16_pairs_supported(nc, p.m, prec))
+        return set_error(QCU_ERR_UNSUPPORTED, "two-RHS packed hop: n_color %d, m %d", nc, p.m);
+    if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");
+    auto go = [&](auto tag) -> int {
+        using S = decltype(tag);
+        switch (p.m) {
+            case 8: return launch16p<3, S, 8>(p, dagger, epi, st);
+            case 12: return launch16p<3, S, 12>(p, dagger, epi, st);
+            default: return launch16p<3, S, 16>(p, dagger, epi, st);
+        }
+    };
+    if (prec == QCU_PRECISION_HALF) return go(__half{});
+    return go(__nv_bfloat16{});
 }
 
 // acc16: accumulate the 8 hops in the storage format (FP16 only); staged: read the links

@@ -15,7 +15,7 @@ import ctypes
 import json
 
 PRECS = {"f64": 2, "f32": 1, "f16": 0, "bf16": 4}
-KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged"]
+KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"]
 
 
 def hop_bytes(vh, nc, m, s):

@@ -146,7 +146,8 @@ def test_mixed_precision_reaches_fp64_true_residual(oracle_lib, sloppy):
     assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-2, atol=1e-15)
 
 
-@pytest.mark.parametrize("kind", [q.HOP_PACKED16, q.HOP_PACKED16_ACC16], ids=["packed16", "packed16_acc16"])
+@pytest.mark.parametrize("kind", [q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_PAIRS],
+                         ids=["packed16", "packed16_acc16", "packed16_pairs"])
 @pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
 def test_mixed_precision_with_packed_hop(oracle_lib, sloppy, kind):
     """The packed 16-bit hop inside the mixed solver: its Schur epilogues and fused

@@ -98,13 +98,13 @@ def _acc16_factor(kind, prec):
 
 
 LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16,
-                q.HOP_PACKED16_STAGED]
-LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged"]
+                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS]
+LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"]
 
 
 @pytest.mark.parametrize("hop_kernel", LOWP_KERNELS, indirect=True, ids=LOWP_IDS)
 @pytest.mark.parametrize("prec", [q.SINGLE, q.HALF, q.BF16])
-@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (2, 32), (3, 17), (8, 16), (6, 5), (3, 1)])
+@pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (4, 8), (2, 32), (3, 17), (8, 16), (6, 5), (3, 1), (3, 8), (3, 16)])
 def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
     L = (8, 4, 4, 4)
     gauge, inp = _problem(L, nc, m, 40 + nc)
@@ -121,8 +121,9 @@ def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
     assert q.lib().qcuGetKernelError(1) == 0
 
 
-@pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_STAGED],
-                         indirect=True, ids=["tcgen05", "packed16", "packed16_acc16", "packed16_staged"])
+@pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_STAGED,
+                                        q.HOP_PACKED16_PAIRS], indirect=True,
+                         ids=["tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"])
 @pytest.mark.parametrize("prec", [q.HALF, q.BF16])
 @pytest.mark.parametrize("L", [(2, 2, 2, 2), (6, 2, 4, 2), (4, 4, 4, 6), (8, 8, 8, 10)])
 def test_low_precision_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel):
