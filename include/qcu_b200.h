@@ -246,8 +246,8 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
  *   PACKED16_PAIRS  as PACKED16 with two RHS per thread (8-byte neighbour loads, links
  *            shared by the pair), SU(3) with m = 8, 12 or 16 (else PACKED16);
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
- *            (n_color, m_rhs, precision), else PACKED16 where it applies and SIMT
- *            otherwise. */
+ *            (n_color, m_rhs, precision), else PACKED16_PAIRS, PACKED16 or SIMT,
+ *            the first that applies. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2

@@ -422,6 +422,24 @@ int launch16d_m(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     return QCU_SUCCESS;
 }
 
+// packed FP32 pair arithmetic (add.rn.f32x2 / sub: sm_100): one instruction per complex add
+__device__ __forceinline__ uint64_t f2_bits(float2 v) {
+    return (uint64_t)__float_as_uint(v.x) | ((uint64_t)__float_as_uint(v.y) << 32);
+}
+__device__ __forceinline__ float2 f2_from(uint64_t u) {
+    return make_float2(__uint_as_float((uint32_t)u), __uint_as_float((uint32_t)(u >> 32)));
+}
+__device__ __forceinline__ void f2_add(float2& a, float2 b) {
+    uint64_t z;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    a = f2_from(z);
+}
+__device__ __forceinline__ void f2_sub(float2& a, float2 b) {
+    uint64_t z;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    a = f2_from(z);
+}
+
 // ---- two RHS per thread (compile-time even m) ----
 // Thread per (half-site, RHS pair j): RHS 2j and 2j+1 sit in one 8-byte word pair of every
 // (spin, colour) row, so each neighbour value is one 8-byte load; the links, their
@@ -476,20 +494,22 @@ __device__ __forceinline__ void h16_hop2(float2 (&acc)[2][4][NC], const uint2* _
         for (int r = 0; r < 2; ++r) {
             const float2 f0 = P::f32(w0[r]), f1 = P::f32(w1[r]);
             float2 (&a)[4][NC] = acc[r];
-            a[0][c].x += f0.x; a[0][c].y += f0.y;
-            a[1][c].x += f1.x; a[1][c].y += f1.y;
+            // spins 0, 1 and the real-coefficient terms of spins 2, 3 as packed pair adds;
+            // the +-i terms swap re and im, which stays scalar
+            f2_add(a[0][c], f0);
+            f2_add(a[1][c], f1);
             if (MU == 0) {
                 a[2][c].x += sg * f1.y; a[2][c].y -= sg * f1.x;
                 a[3][c].x += sg * f0.y; a[3][c].y -= sg * f0.x;
             } else if (MU == 1) {
-                a[2][c].x += sg * f1.x; a[2][c].y += sg * f1.y;
-                a[3][c].x -= sg * f0.x; a[3][c].y -= sg * f0.y;
+                if (SG > 0) { f2_add(a[2][c], f1); f2_sub(a[3][c], f0); }
+                else { f2_sub(a[2][c], f1); f2_add(a[3][c], f0); }
             } else if (MU == 2) {
                 a[2][c].x += sg * f0.y; a[2][c].y -= sg * f0.x;
                 a[3][c].x -= sg * f1.y; a[3][c].y += sg * f1.x;
             } else {
-                a[2][c].x += sg * f0.x; a[2][c].y += sg * f0.y;
-                a[3][c].x += sg * f1.x; a[3][c].y += sg * f1.y;
+                if (SG > 0) { f2_add(a[2][c], f0); f2_add(a[3][c], f1); }
+                else { f2_sub(a[2][c], f0); f2_sub(a[3][c], f1); }
             }
         }
     }

@@ -60,8 +60,10 @@ int auto_hop_kind(int nc, int m, int prec) {
         auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
         if (it != g_tuned.end()) return it->second;
     }
-    // measured on B200 (16^4, N = 3..8, m = 8..32): packed 16-bit arithmetic wins for
-    // FP16/BF16 storage wherever it applies, the per-(site, RHS) SIMT kernel everywhere else
+    // measured on B200 (16^4 and 24^3x48, N = 3..8, m = 8..32): packed 16-bit arithmetic
+    // wins for FP16/BF16 storage wherever it applies (two RHS per thread where that is
+    // specialised), the per-(site, RHS) SIMT kernel everywhere else
+    if (hop16_pairs_supported(nc, m, prec)) return QCU_HOP_PACKED16_PAIRS;
     if (hop16_supported(nc, m, prec)) return QCU_HOP_PACKED16;
     return QCU_HOP_SIMT;
 }
