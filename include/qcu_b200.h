@@ -227,6 +227,12 @@ int qcuElementwiseInit(void *res, double re, double im, int m, void *stream);
  * (gauge_eo_precondition without a context). */
 int qcuGaugeToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
 int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
+/* Fermion reorder lexicographic [Lt][Lz][Ly][Lx][4][Nc] <-> even/odd [2][Vh][4][Nc] (one RHS).
+ * The reference keeps this conversion in its external submodule (absent from its tree);
+ * the even/odd convention is the one of include/point/qcu_point.cuh:16-61 (parity
+ * (x+y+z+t) mod 2, x = 2*xh + ((p+y+z+t) & 1)). */
+int qcuFermionToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
+int qcuFermionFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
 
 /* Hop kernel selection.
  *   SIMT     one thread per (site, RHS), all colours in registers;

@@ -129,6 +129,8 @@ _SIGNATURES = {
     "qcuElementwiseInit": (_i, [_vp, _d, _d, _i, _vp]),
     "qcuGaugeToEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
     "qcuGaugeFromEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
+    "qcuFermionToEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
+    "qcuFermionFromEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
     "qcuSetHopKernel": (_i, [_i]),
     "qcuGetHopKernel": (_i, []),
     "qcuGetKernelError": (_i, [_i]),

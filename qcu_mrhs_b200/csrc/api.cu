@@ -609,6 +609,20 @@ int qcuGaugeFromEO(void* lex, const void* eo, const int L[4], int n_color, int p
     return gauge_reorder(lex, eo, L, n_color, precision, 0, static_cast<cudaStream_t>(stream));
 }
 
+int qcuFermionToEO(void* eo, const void* lex, const int L[4], int n_color, int precision, void* stream) {
+    clear_error();
+    if (!eo || !lex || !L) return set_error(QCU_ERR_INVALID, "null pointer");
+    if (n_color < 1 || n_color > kMaxColor) return set_error(QCU_ERR_INVALID, "n_color=%d", n_color);
+    return fermion_reorder(eo, lex, L, n_color, precision, 1, static_cast<cudaStream_t>(stream));
+}
+
+int qcuFermionFromEO(void* lex, const void* eo, const int L[4], int n_color, int precision, void* stream) {
+    clear_error();
+    if (!eo || !lex || !L) return set_error(QCU_ERR_INVALID, "null pointer");
+    if (n_color < 1 || n_color > kMaxColor) return set_error(QCU_ERR_INVALID, "n_color=%d", n_color);
+    return fermion_reorder(lex, eo, L, n_color, precision, 0, static_cast<cudaStream_t>(stream));
+}
+
 int qcuSetHopKernel(int kind) {
     clear_error();
     if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_PAIRS)

@@ -92,21 +92,23 @@ __global__ void cast_kernel(typename St<D>::S2* __restrict__ dst, const typename
 }
 
 // lexicographic [4][Lt][Lz][Ly][Lx][N][N] <-> even/odd [4][2][Vh][N][N]
+// Site reorder between lexicographic [nblk][Lt][Lz][Ly][Lx][per_site] and even/odd
+// [nblk][2][Vh][per_site] (parity (x+y+z+t) mod 2, full x = 2 xh + ((p + y + z + t) & 1)):
+// the gauge field has 4 blocks (directions) of N*N per site, a fermion 1 block of 4*N.
 template <typename S>
-__global__ void gauge_reorder_kernel(typename St<S>::S2* __restrict__ dst,
-                                     const typename St<S>::S2* __restrict__ src, Geom g, int n2,
-                                     int to_eo) {
+__global__ void site_reorder_kernel(typename St<S>::S2* __restrict__ dst, const typename St<S>::S2* __restrict__ src,
+                                    Geom g, int per_site, int nblk, int to_eo) {
     const int64_t V = 2 * g.vh;
-    const int64_t total = 4 * V * n2;
+    const int64_t total = (int64_t)nblk * V * per_site;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         // i indexes the even/odd array
-        const int e = (int)(i % n2);
-        int64_t q = i / n2;
+        const int e = (int)(i % per_site);
+        int64_t q = i / per_site;
         const int64_t hidx = q % g.vh;
         q /= g.vh;
         const int par = (int)(q % 2);
-        const int mu = (int)(q / 2);
+        const int blk = (int)(q / 2);
         int64_t h = hidx;
         const int xh = (int)(h % g.lxh); h /= g.lxh;
         const int y = (int)(h % g.L[1]); h /= g.L[1];
@@ -114,7 +116,7 @@ __global__ void gauge_reorder_kernel(typename St<S>::S2* __restrict__ dst,
         const int t = (int)(h / g.L[2]);
         const int x = 2 * xh + ((par + y + z + t) & 1);
         const int64_t lex = (((int64_t)t * g.L[2] + z) * g.L[1] + y) * g.L[0] + x;
-        const int64_t li = ((int64_t)mu * V + lex) * n2 + e;
+        const int64_t li = ((int64_t)blk * V + lex) * per_site + e;
         if (to_eo) dst[i] = src[li];
         else dst[li] = src[i];
     }
@@ -197,20 +199,29 @@ int cast_complex(void* dst, int dprec, const void* src, int sprec, int64_t n, cu
     });
 }
 
-int gauge_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo,
-                  cudaStream_t st) {
-    if (L[0] % 2) return set_error(QCU_ERR_INVALID, "Lx must be even");
-    if (dst == src) return set_error(QCU_ERR_INVALID, "in-place gauge reorder is not supported");
+static int site_reorder(void* dst, const void* src, const int L[4], int per_site, int nblk, int prec, int to_eo,
+                        cudaStream_t st) {
+    if (L[0] < 2 || L[0] % 2 || L[1] < 1 || L[2] < 1 || L[3] < 1)
+        return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", L[0], L[1], L[2], L[3]);
+    if (dst == src) return set_error(QCU_ERR_INVALID, "in-place reorder is not supported");
     const Geom g = make_geom(L);
     return dispatch_prec(prec, [&](auto tag) {
         using S = decltype(tag);
-        auto k = gauge_reorder_kernel<S>;
-        const int grid = resident_grid(k, 256, 8 * g.vh * nc * nc);
-        k<<<grid, 256, 0, st>>>(static_cast<typename St<S>::S2*>(dst),
-                                static_cast<const typename St<S>::S2*>(src), g, nc * nc, to_eo);
+        auto k = site_reorder_kernel<S>;
+        const int grid = resident_grid(k, 256, 2 * g.vh * nblk * per_site);
+        k<<<grid, 256, 0, st>>>(static_cast<typename St<S>::S2*>(dst), static_cast<const typename St<S>::S2*>(src), g,
+                                per_site, nblk, to_eo);
         QCUB_CHECK_LAUNCH();
         return QCU_SUCCESS;
     });
+}
+
+int gauge_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo, cudaStream_t st) {
+    return site_reorder(dst, src, L, nc * nc, 4, prec, to_eo, st);
+}
+
+int fermion_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo, cudaStream_t st) {
+    return site_reorder(dst, src, L, 4 * nc, 1, prec, to_eo, st);
 }
 
 }  // namespace qcub

@@ -14,5 +14,7 @@ int cast_complex(void* dst, int dprec, const void* src, int sprec, int64_t n, cu
 // to_eo = 1: lexicographic -> even/odd; 0: even/odd -> lexicographic
 int gauge_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo,
                   cudaStream_t st);
+// fermion [Lt][Lz][Ly][Lx][4][nc] <-> [2][Vh][4][nc]
+int fermion_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo, cudaStream_t st);
 
 }  // namespace qcub

@@ -151,3 +151,23 @@ def test_gauge_eo_reorder(oracle_lib, prec):
     q.check(q.lib().qcuGaugeFromEO(back.data_ptr(), de.data_ptr(), q.lattice(L), nc, prec, None))
     sync()
     assert np.array_equal(from_dev(back), from_dev(dl))
+
+
+@pytest.mark.parametrize("prec", [q.DOUBLE, q.SINGLE, q.HALF])
+@pytest.mark.parametrize("L", [(4, 2, 6, 2), (2, 4, 2, 4), (6, 6, 4, 8)])
+def test_fermion_eo_reorder(oracle_lib, prec, L):
+    """Lexicographic <-> even/odd fermion order against the oracle; exact (a permutation)."""
+    nc = 3
+    V = L[0] * L[1] * L[2] * L[3]
+    rng = np.random.default_rng(81)
+    lex = rng.standard_normal((V, 4, nc)) + 1j * rng.standard_normal((V, 4, nc))
+    dl = to_dev(lex, prec)
+    de = empty_dev(lex.shape, prec)
+    q.check(q.lib().qcuFermionToEO(de.data_ptr(), dl.data_ptr(), q.lattice(L), nc, prec, None))
+    sync()
+    ref = oracle_lib.fermion_to_eo(from_dev(dl), L)
+    assert np.array_equal(from_dev(de).reshape(ref.shape), ref)
+    back = empty_dev(lex.shape, prec)
+    q.check(q.lib().qcuFermionFromEO(back.data_ptr(), de.data_ptr(), q.lattice(L), nc, prec, None))
+    sync()
+    assert np.array_equal(from_dev(back), from_dev(dl))

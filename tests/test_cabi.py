@@ -108,3 +108,9 @@ def test_precond_rejects_bad_arguments_without_a_gpu(qlib):
     assert lib.qcuPrecondCreate(C.byref(h), qlib.lattice((8, 4, 4, 4)), 3, 4, 4, 8, 0.5) == qlib.ERR_INVALID
     assert not h.value
     assert lib.qcuPrecondApply(None, None, None, qlib.DOUBLE, None) == qlib.ERR_INVALID
+
+
+def test_fermion_reorder_rejects_bad_arguments_without_a_gpu(qlib):
+    lib = qlib.lib()
+    assert lib.qcuFermionToEO(None, None, qlib.lattice((4, 4, 4, 4)), 3, qlib.DOUBLE, None) == qlib.ERR_INVALID
+    assert lib.qcuFermionFromEO(1, 2, qlib.lattice((4, 4, 4, 4)), 0, qlib.DOUBLE, None) == qlib.ERR_INVALID
