@@ -51,6 +51,8 @@ const char *qcuGetLastError(void);
 #define QCU_SOLVER_PRECOND 3   /* FP64 BiCGStab on the full system, right-preconditioned by the
                                   learned preconditioner of qcuSetPreconditioner; falls back to
                                   QCU_SOLVER_FUSED if it does not converge */
+#define QCU_SOLVER_CGNR 4      /* conjugate gradients on the normal equations of the Schur
+                                  system, A^dag A x = A^dag b' (A^dag from the dagger hops) */
 
 typedef struct {
     int solver;              /* QCU_SOLVER_* (default QCU_SOLVER_FUSED) */

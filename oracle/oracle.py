@@ -172,6 +172,57 @@ def bicgstab(b_mrhs_full, gauge, L, kappa, max_iter, tol, t_sign=1.0):
     return x, int(it), rr
 
 
+def cgnr(b_mrhs_full, gauge, L, kappa, max_iter, tol, t_sign=1.0, true_rule=False):
+    """CG on the normal equations of the Schur system, A^dag A x_o = A^dag b'_o, with
+    A = 1 - kappa^2 D_oe D_eo and A^dag from the dagger hops; per-RHS alpha and beta.
+    Stops when every RHS has ||b' - A x_o|| <= tol ||b'|| (||b|| of the full system with
+    true_rule).  The reference has no normal-equation solver: this restates textbook CGNR
+    on the reference's hop (oracle_hop_mrhs) as the checker of the library's
+    QCU_SOLVER_CGNR.  b: gathered full lattice [2][Vh][4][N][m].
+    Returns (x, iterations or -1, per-RHS ||b' - A x_o|| / reference norm)."""
+    b = _c(b_mrhs_full)
+    m = b.shape[4]
+    k2 = kappa * kappa
+
+    def op(v, dag):
+        t = hop(v, gauge, L, 0, dag, t_sign)
+        return v - k2 * hop(t, gauge, L, 1, dag, t_sign)
+
+    def dot(a, c):
+        return np.einsum("vsci,vsci->i", a.conj(), c).real
+
+    be, bo = b[0], b[1]
+    bp = bo + kappa * hop(be, gauge, L, 1, False, t_sign)
+    ref = dot(be, be) + dot(bo, bo) if true_rule else dot(bp, bp)
+    x = np.zeros_like(bp)
+    s = bp.copy()
+    r = op(bp, True)
+    p = r.copy()
+    rr = dot(r, r)
+    it = 0
+    ss = dot(s, s)
+    while not np.all(ss <= tol * tol * ref):
+        if it >= max_iter:
+            it = -1
+            break
+        q = op(p, False)
+        z = op(q, True)
+        qq = dot(q, q)
+        alpha = np.where(qq > 0, rr / np.where(qq > 0, qq, 1.0), 0.0)
+        x = x + alpha * p
+        s = s - alpha * q
+        r = r - alpha * z
+        rrn = dot(r, r)
+        beta = np.where(rr > 0, rrn / np.where(rr > 0, rr, 1.0), 0.0)
+        rr = rrn
+        p = r + beta * p
+        ss = dot(s, s)
+        it += 1
+    xe = be + kappa * hop(x, gauge, L, 0, False, t_sign)
+    rel = np.sqrt(ss / np.where(ref > 0, ref, 1.0))
+    return np.stack([xe, x]), it, rel
+
+
 def gauge_to_eo(lex, L):
     lex = _c(lex)
     nc = lex.shape[-1]

@@ -22,7 +22,7 @@ PREC_BYTES = {HALF: 2, SINGLE: 4, DOUBLE: 8, BF16: 2}
 # status codes
 SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_UNSUPPORTED, ERR_ALLOC = range(8)
 
-SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND = 0, 1, 2, 3
+SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND, SOLVER_CGNR = 0, 1, 2, 3, 4
 (HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16, HOP_PACKED16_STAGED,
  HOP_PACKED16_PAIRS) = range(8)
 MAX_RHS = 64

@@ -308,6 +308,8 @@ static int invert_impl(int max_iter, double tol) {
     c.stats = QcuSolveStats{};
     if (c.opts.solver == QCU_SOLVER_PRECOND)
         rc = solve_precond(c, c.precond, x, b, max_iter, tol);
+    else if (c.opts.solver == QCU_SOLVER_CGNR)
+        rc = solve_cgnr(c, x, b, max_iter, tol);
     else
         rc = mixed ? solve_mixed(c, x, b, max_iter, tol) : solve_fused(c, x, b, max_iter, tol);
     const int solve_rc = rc;
@@ -418,7 +420,7 @@ int qcuSetSolverOptions(const QcuSolverOptions* opts) {
     int rc = require_ctx();
     if (rc) return rc;
     if (!opts) return set_error(QCU_ERR_INVALID, "null options");
-    if (opts->solver < QCU_SOLVER_REFERENCE || opts->solver > QCU_SOLVER_PRECOND)
+    if (opts->solver < QCU_SOLVER_REFERENCE || opts->solver > QCU_SOLVER_CGNR)
         return set_error(QCU_ERR_INVALID, "solver %d", opts->solver);
     if (opts->t_boundary != 1.0 && opts->t_boundary != -1.0)
         return set_error(QCU_ERR_INVALID, "t_boundary must be +1 or -1");

@@ -98,6 +98,7 @@ class SchurSolve {
 // Whole solves (solver.cu): begin, iterations in graphs of check_interval, end.
 int solve_fused(Context& c, void* x, const void* b, int max_iter, double tol);
 int solve_mixed(Context& c, void* x, const void* b, int max_iter, double tol);
+int solve_cgnr(Context& c, void* x, const void* b, int max_iter, double tol);
 
 // Context life cycle (api.cu), shared by the qcu.h object and the batched solver.
 int context_init(Context* c, const int L[4], int n_color, int m_rhs, int in_prec, int dslash_prec);

@@ -140,6 +140,21 @@ int true_residual(Context& c, int prec, const void* gauge, const void* x, const 
     return QCU_SUCCESS;
 }
 
+// alpha_j = rr_j / qq_j (0 for a finished or zero right-hand side)
+__global__ void cg_alpha_kernel(double2* alpha, const double2* rr, const double2* qq, int m) {
+    const int j = threadIdx.x;
+    if (j >= m) return;
+    alpha[j] = make_double2(qq[j].x > 0.0 ? rr[j].x / qq[j].x : 0.0, 0.0);
+}
+
+// beta_j = rr_new_j / rr_j ; rr_j <- rr_new_j
+__global__ void cg_beta_kernel(double2* beta, double2* rr, const double2* rr_new, int m) {
+    const int j = threadIdx.x;
+    if (j >= m) return;
+    beta[j] = make_double2(rr[j].x > 0.0 ? rr_new[j].x / rr[j].x : 0.0, 0.0);
+    rr[j] = rr_new[j];
+}
+
 int finish_stats(Context& c, int prec, const void* gauge, const void* x, const void* b, void* tmp,
                  double2* slots) {
     QcuSolveStats& st = c.stats;
@@ -345,6 +360,123 @@ int solve_fused(Context& c, void* x, const void* b, int max_iter, double tol) {
 
 int solve_mixed(Context& c, void* x, const void* b, int max_iter, double tol) {
     return solve_one(c, x, b, max_iter, tol, true);
+}
+
+// CGNR on the even/odd Schur system: conjugate gradients on A^dag A x_o = A^dag b'_o with
+// A = 1 - kappa^2 D_oe D_eo and A^dag = 1 - kappa^2 (D^dag)_oe (D^dag)_eo (the dagger hops).
+// The Schur residual s = b' - A x_o is carried along (s -= alpha A p), so the stopping rules
+// are those of the BiCGStab solvers: ||s_j|| <= tol ||b'_j|| for every RHS, or the
+// full-system ||b_j|| with stop_true_residual.  The host reads the residual norms every
+// iteration.
+int solve_cgnr(Context& c, void* x, const void* b, int max_iter, double tol) {
+    const int P = c.in_prec;
+    if (P != QCU_PRECISION_DOUBLE && P != QCU_PRECISION_SINGLE)
+        return set_error(QCU_ERR_UNSUPPORTED, "the CGNR solve needs double or single precision fields");
+    const void* g = nullptr;
+    int rc;
+    if ((rc = c.gauge_in(P, &g))) return rc;
+    const size_t hb = c.half_bytes(P);
+    void* v_[7];
+    for (int i = 0; i < 7; ++i) {
+        if ((rc = c.sv[i].ensure(hb))) return rc;
+        v_[i] = c.sv[i].ptr;
+    }
+    if ((rc = c.sv[15].ensure(sizeof(double2) * 8 * kMaxRhs))) return rc;
+    double2* sl = static_cast<double2*>(c.sv[15].ptr);
+    double2 *rr = sl, *qq = sl + kMaxRhs, *alpha = sl + 2 * kMaxRhs, *beta = sl + 3 * kMaxRhs;
+    double2 *rrn = sl + 4 * kMaxRhs, *ss = sl + 5 * kMaxRhs, *bb = sl + 6 * kMaxRhs, *be2 = sl + 7 * kMaxRhs;
+    void* bp = v_[0]; void* sres = v_[1]; void* r = v_[2]; void* p = v_[3]; void* qv = v_[4]; void* z = v_[5];
+    void* tmp = v_[6];
+    const char* be = static_cast<const char*>(b);
+    const void* bo = be + hb;
+    char* xe = static_cast<char*>(x);
+    void* xo = xe + hb;
+    const int64_t len = c.half_len();
+    const int m = c.m;
+    const double k2 = c.kappa * c.kappa;
+    const cudaStream_t st = c.stream;
+    auto hop = [&](void* out, const void* in, int parity, bool dag, int epi, const void* xv, double a) -> int {
+        HopParams hp{};
+        hp.out = out; hp.in = in; hp.gauge = g; hp.x = xv; hp.a = a;
+        hp.g = c.g; hp.m = m; hp.parity = parity; hp.t_sign = c.opts.t_boundary;
+        hp.red = RedArgs{c.ws.partials, c.ws.counter, c.ws.result, nullptr, nullptr, FIN_NONE};
+        return hop_launch(hp, c.nc, P, dag, epi, st);
+    };
+    // A v (dag = false) or A^dag v (dag = true) into out, through tmp
+    auto schur = [&](void* out, const void* in, bool dag) -> int {
+        int e;
+        if ((e = hop(tmp, in, 0, dag, EPI_PLAIN, nullptr, 0.0))) return e;
+        return hop(out, tmp, 1, dag, EPI_XPAY, in, -k2);
+    };
+    QCUB_CUDA_CHECK(cudaEventRecord(c.ev0, st));
+    // b' = b_o + kappa D_oe b_e ; s = b' ; r = p = A^dag b' ; x_o = 0
+    if ((rc = hop(bp, be, 1, false, EPI_XPAY, bo, c.kappa))) return rc;
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(sres, bp, hb, cudaMemcpyDeviceToDevice, st));
+    if ((rc = schur(r, bp, true))) return rc;
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(p, r, hb, cudaMemcpyDeviceToDevice, st));
+    QCUB_CUDA_CHECK(cudaMemsetAsync(xo, 0, hb, st));
+    if ((rc = mrhs_dotc(rr, r, r, len, m, P, c.ws, st))) return rc;
+    if ((rc = mrhs_dotc(bb, bp, bp, len, m, P, c.ws, st))) return rc;
+    if ((rc = mrhs_dotc(be2, be, be, len, m, P, c.ws, st))) return rc;
+    if ((rc = mrhs_dotc(qq, bo, bo, len, m, P, c.ws, st))) return rc;   // ||b_o||^2, reused below
+    double2 h[3 * kMaxRhs];
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(h, bb, sizeof(double2) * kMaxRhs, cudaMemcpyDeviceToHost, st));
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(h + kMaxRhs, be2, sizeof(double2) * kMaxRhs, cudaMemcpyDeviceToHost, st));
+    QCUB_CUDA_CHECK(cudaMemcpyAsync(h + 2 * kMaxRhs, qq, sizeof(double2) * kMaxRhs, cudaMemcpyDeviceToHost, st));
+    QCUB_CUDA_CHECK(cudaStreamSynchronize(st));
+    double ref2[kMaxRhs];   // stopping reference ||b'||^2 or ||b||^2 per RHS
+    for (int j = 0; j < m; ++j)
+        ref2[j] = c.opts.stop_true_residual ? h[kMaxRhs + j].x + h[2 * kMaxRhs + j].x : h[j].x;
+    int it = 0, status = 3;
+    double sn2[kMaxRhs];
+    for (int j = 0; j < m; ++j) sn2[j] = h[j].x;
+    auto converged = [&]() {
+        for (int j = 0; j < m; ++j)
+            if (sn2[j] > tol * tol * ref2[j]) return false;
+        return true;
+    };
+    if (converged()) status = 1;
+    while (status == 3 && it < max_iter) {
+        if ((rc = schur(qv, p, false))) return rc;       // q = A p
+        if ((rc = schur(z, qv, true))) return rc;        // z = A^dag q
+        if ((rc = mrhs_dotc(qq, qv, qv, len, m, P, c.ws, st))) return rc;
+        cg_alpha_kernel<<<1, kMaxRhs, 0, st>>>(alpha, rr, qq, m);
+        QCUB_CHECK_LAUNCH();
+        if ((rc = mrhs_axpy(OP_XPAY, xo, alpha, xo, nullptr, p, nullptr, nullptr, len, m, P, st))) return rc;
+        if ((rc = mrhs_axpy(OP_XSAY, sres, alpha, sres, nullptr, qv, nullptr, nullptr, len, m, P, st))) return rc;
+        if ((rc = mrhs_axpy(OP_XSAY, r, alpha, r, nullptr, z, nullptr, nullptr, len, m, P, st))) return rc;
+        if ((rc = mrhs_dotc(rrn, r, r, len, m, P, c.ws, st))) return rc;
+        cg_beta_kernel<<<1, kMaxRhs, 0, st>>>(beta, rr, rrn, m);
+        QCUB_CHECK_LAUNCH();
+        if ((rc = mrhs_axpy(OP_XPAY, p, beta, r, nullptr, p, nullptr, nullptr, len, m, P, st))) return rc;
+        if ((rc = mrhs_dotc(ss, sres, sres, len, m, P, c.ws, st))) return rc;
+        QCUB_CUDA_CHECK(cudaMemcpyAsync(h, ss, sizeof(double2) * kMaxRhs, cudaMemcpyDeviceToHost, st));
+        QCUB_CUDA_CHECK(cudaStreamSynchronize(st));
+        ++it;
+        for (int j = 0; j < m; ++j) sn2[j] = h[j].x;
+        bool finite = true;
+        for (int j = 0; j < m; ++j) finite = finite && std::isfinite(sn2[j]);
+        if (!finite) status = 2;
+        else if (converged()) status = 1;
+    }
+    // x_e = b_e + kappa D_eo x_o
+    if ((rc = hop(xe, xo, 0, false, EPI_XPAY, be, c.kappa))) return rc;
+    QCUB_CUDA_CHECK(cudaEventRecord(c.ev1, st));
+    c.host_sc->iter = it;
+    c.host_sc->reliable = 0;
+    c.host_sc->status = status;
+    for (int j = 0; j < m; ++j) {
+        c.host_sc->bnorm2[j] = ref2[j];
+        c.host_sc->rnorm2[j] = sn2[j];
+    }
+    if ((rc = finish_stats(c, P, g, x, b, tmp, sl))) return rc;
+    float ms = 0.f;
+    QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+    c.stats.solve_seconds = ms * 1e-3;
+    if (c.stats.status != QCU_SUCCESS)
+        return set_error(c.stats.status, "CGNR stopped after %d iterations (%s)", it,
+                         c.stats.status == QCU_ERR_BREAKDOWN ? "breakdown" : "max_iteration reached");
+    return QCU_SUCCESS;
 }
 
 // Right-preconditioned BiCGStab on the full system M (P y) = b, x = P y, in FP64 with P

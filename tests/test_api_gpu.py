@@ -166,6 +166,70 @@ def test_mixed_precision_with_packed_hop(oracle_lib, sloppy, kind):
     assert np.all(true_rel <= tol)
 
 
+@pytest.mark.parametrize("true_rule", [0, 1], ids=["schur_rule", "true_rule"])
+def test_cgnr_matches_oracle(oracle_lib, true_rule):
+    """QCU_SOLVER_CGNR: CG on A^dag A x = A^dag b' follows the oracle's CGNR iterate by
+    iterate (same iteration count within one, same solution), meets its stopping rule,
+    and reports the FP64 true residual the oracle recomputes; the solution agrees with
+    the BiCGStab one."""
+    L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 4, 0.10, 1e-10
+    gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 30, t_boundary=-1.0,
+                                     opts={"solver": q.SOLVER_CGNR, "stop_true_residual": true_rule})
+    assert st == q.SUCCESS, q.last_error()
+    bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
+    xo, it, rr = oracle_lib.cgnr(bm, gauge, L, kappa, 2000, tol, t_sign=-1.0, true_rule=bool(true_rule))
+    assert it > 0 and abs(stats.iterations - it) <= 1
+    xref = np.stack([F.from_mrhs(xo[0]), F.from_mrhs(xo[1])], axis=1)
+    assert rel_err(x, xref) <= 1e-8
+    assert np.all(np.array(stats.recursive_residual[:m]) <= tol)
+    res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.all(true_rel <= 10 * tol)
+    assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-2, atol=1e-14)
+    xb, itb, _ = oracle_lib.bicgstab(bm, gauge, L, kappa, 2000, tol, t_sign=-1.0)
+    xbr = np.stack([F.from_mrhs(xb[0]), F.from_mrhs(xb[1])], axis=1)
+    assert rel_err(x, xbr) <= 1e-8
+
+
+def test_cgnr_single_precision(oracle_lib):
+    """FP32 fields through CGNR: converges to the FP32-reachable tolerance."""
+    L, nc, m, kappa, tol = (8, 4, 4, 8), 3, 3, 0.12, 1e-5
+    init(L, nc, m, q.SINGLE, q.SINGLE)
+    gauge = F.gauge_field(L, nc, 31, kind="smooth", eps=0.3)
+    dg = to_dev(gauge, q.SINGLE)
+    q.lib().loadQcuGauge(dg.data_ptr(), q.SINGLE)
+    q.lib().getDslash(0, 1.0 / (2 * kappa) - 4.0)
+    o = q.default_options()
+    o.solver = q.SOLVER_CGNR
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    vh = F.half_volume(L)
+    b = F.gaussian_fermions(L, nc, m, 32)
+    ins = [to_dev(b[j], q.SINGLE) for j in range(m)]
+    outs = [empty_dev((2, vh, 4, nc), q.SINGLE) for _ in range(m)]
+    for j in range(m):
+        q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+    q.lib().qcuInvert(2000, tol)
+    assert q.status() == q.SUCCESS, q.last_error()
+    x = np.stack([from_dev(t) for t in outs])
+    b32 = np.stack([from_dev(t) for t in ins])
+    res = oracle_lib.mat(x, gauge, L, kappa) - b32
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b32.reshape(m, -1), axis=1)
+    assert np.all(true_rel <= 10 * tol)
+
+
+def test_cgnr_not_converged_and_options():
+    L, nc, m, kappa = (4, 4, 4, 4), 3, 2, 0.12
+    _, _, _, st, stats = _invert(L, nc, m, kappa, 1e-12, 40, max_iter=3, opts={"solver": q.SOLVER_CGNR})
+    assert st == q.ERR_NOT_CONVERGED
+    assert stats.iterations == 3
+    o = q.default_options()
+    o.solver = q.SOLVER_CGNR + 1
+    assert q.lib().qcuSetSolverOptions(ctypes.byref(o)) == q.ERR_INVALID
+    o.solver = q.SOLVER_CGNR
+    init(L, nc, m, q.HALF, q.HALF)
+    assert q.lib().qcuSetSolverOptions(ctypes.byref(o)) == q.SUCCESS
+
+
 def test_invert_not_converged_status():
     L, nc, m = (4, 4, 4, 4), 3, 2
     gauge, b, x, st, stats = _invert(L, nc, m, 0.12, 1e-14, 16, max_iter=3)

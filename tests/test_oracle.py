@@ -195,6 +195,25 @@ def test_bicgstab_solves_full_system(oracle_lib):
     assert np.linalg.norm(res) / np.linalg.norm(psi) < 1e-11
 
 
+def test_cgnr_solves_full_system(oracle_lib):
+    """The oracle's CGNR (the checker of QCU_SOLVER_CGNR) reaches the same solution as
+    the Schur BiCGStab and the FP64 true residual it claims."""
+    O = oracle_lib
+    L = (4, 4, 4, 4)
+    kappa = 0.12
+    gauge, psi = _random_problem(L, 3, 3, 7)
+    b = np.stack([F.to_mrhs(psi[:, 0]), F.to_mrhs(psi[:, 1])])
+    x, it, rr = O.cgnr(b, gauge, L, kappa, 2000, 1e-12)
+    assert it > 0 and np.all(rr <= 1e-12)
+    xb, _, _ = O.bicgstab(b, gauge, L, kappa, 500, 1e-12)
+    assert np.linalg.norm(x - xb) / np.linalg.norm(xb) < 1e-10
+    xr = np.stack([F.from_mrhs(x[0]), F.from_mrhs(x[1])], axis=1)
+    res = O.mat(xr, gauge, L, kappa) - psi
+    assert np.linalg.norm(res) / np.linalg.norm(psi) < 1e-11
+    _, it0, _ = O.cgnr(b, gauge, L, kappa, 0, 1e-12)
+    assert it0 == -1
+
+
 def test_bicgstab_zero_iterations_and_zero_source(oracle_lib):
     O = oracle_lib
     L = (4, 2, 2, 2)
