@@ -236,6 +236,21 @@ int qcuGaugeFromEO(void *lex, const void *eo, const int L[4], int n_color, int p
 int qcuFermionToEO(void *eo, const void *lex, const int L[4], int n_color, int precision, void *stream);
 int qcuFermionFromEO(void *lex, const void *eo, const int L[4], int n_color, int precision, void *stream);
 
+/* Site-blocked layout of a multi-RHS half-lattice field (no reference counterpart): the
+ * layout the mixed solver keeps its 16-bit vectors in.  Blocks of 32 sites; inside a block
+ * the 4 Nc spin-colour rows one after another, each row holding the block's 32 sites with
+ * their m right-hand sides innermost:
+ *   complex (site n, row r, RHS j) at ((n / 32) 4 Nc + r) 32 m + (n % 32) m + j.
+ * A warp reading one row of consecutive sites reads one contiguous run.
+ * qcuSiteBlockMrhs reorders gathered [Vh][4][Nc][m] -> blocked (to_blocked = 1) or back
+ * (0), not in place; vh must be a multiple of 32.
+ * qcuDslashMrhsSiteBlocked is qcuDslashMrhs on blocked in/out: FP16 or BF16, SU(3),
+ * m = 8, 12 or 16, vh a multiple of 32. */
+int qcuSiteBlockMrhs(void *dst, const void *src, int64_t vh, int n_color, int m_rhs, int precision,
+                     int to_blocked, void *stream);
+int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const int L[4], int n_color,
+                             int m_rhs, int parity, int dagger, double t_sign, int precision, void *stream);
+
 /* Hop kernel selection.
  *   SIMT     one thread per (site, RHS), all colours in registers;
  *   SIMT_CS  one thread per (site, RHS, colour): fewer registers (FP64, large N),

@@ -131,6 +131,8 @@ _SIGNATURES = {
     "qcuGaugeFromEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
     "qcuFermionToEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
     "qcuFermionFromEO": (_i, [_vp, _vp, _ip, _i, _i, _vp]),
+    "qcuSiteBlockMrhs": (_i, [_vp, _vp, ctypes.c_int64, _i, _i, _i, _i, _vp]),
+    "qcuDslashMrhsSiteBlocked": (_i, [_vp, _vp, _vp, _ip, _i, _i, _i, _i, ctypes.c_double, _i, _vp]),
     "qcuSetHopKernel": (_i, [_i]),
     "qcuGetHopKernel": (_i, []),
     "qcuGetKernelError": (_i, [_i]),

@@ -625,6 +625,30 @@ int qcuFermionFromEO(void* lex, const void* eo, const int L[4], int n_color, int
     return fermion_reorder(lex, eo, L, n_color, precision, 0, static_cast<cudaStream_t>(stream));
 }
 
+int qcuSiteBlockMrhs(void* dst, const void* src, int64_t vh, int n_color, int m_rhs, int precision,
+                     int to_blocked, void* stream) {
+    clear_error();
+    if (to_blocked != 0 && to_blocked != 1) return set_error(QCU_ERR_INVALID, "to_blocked %d", to_blocked);
+    return site_block_reorder(dst, src, vh, n_color, m_rhs, precision, to_blocked, static_cast<cudaStream_t>(stream));
+}
+
+int qcuDslashMrhsSiteBlocked(void* out, const void* in, const void* gauge, const int L[4], int n_color, int m_rhs,
+                             int parity, int dagger, double t_sign, int precision, void* stream) {
+    clear_error();
+    if (!out || !in || !gauge || !L) return set_error(QCU_ERR_INVALID, "null pointer");
+    if (parity != 0 && parity != 1) return set_error(QCU_ERR_INVALID, "parity %d", parity);
+    HopParams p{};
+    p.out = out;
+    p.in = in;
+    p.gauge = gauge;
+    p.g = make_geom(L);
+    p.m = m_rhs;
+    p.parity = parity;
+    p.t_sign = t_sign;
+    p.blocked = 1;
+    return hop_launch(p, n_color, precision, dagger != 0, EPI_PLAIN, static_cast<cudaStream_t>(stream));
+}
+
 int qcuSetHopKernel(int kind) {
     clear_error();
     if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_PAIRS)

@@ -21,6 +21,22 @@ constexpr int kNs = 4;          // spin components
 constexpr int kNd = 4;          // space-time dimensions
 constexpr int kMaxColor = 8;    // largest N with a compiled kernel
 constexpr int kMaxRhs = 64;     // largest m (per call) supported by the kernels
+// Site-blocked spinor layout (the mixed solver's 16-bit vectors): blocks of kSiteBlock
+// half-lattice sites; inside a block the 4N spin-colour rows one after another, each row
+// holding the block's sites with their m right-hand sides innermost:
+//   complex (site n, row r, RHS j) at ((n / kSiteBlock) 4N + r) kSiteBlock m + (n % kSiteBlock) m + j.
+// A warp's load of one row of consecutive sites is then one contiguous run.
+constexpr int kSiteBlock = 32;
+
+// Site-blocked complex index of gathered index gi = (site rows + row) m + j, rows = 4N
+// (fewer than 2^31 complex in all).
+__device__ __forceinline__ int64_t site_blocked_index(int64_t gi, int m, int rows) {
+    const uint32_t g = (uint32_t)gi, um = (uint32_t)m, ur = (uint32_t)rows;
+    const uint32_t q = g / um, j = g - q * um;
+    const uint32_t n = q / ur, r = q - n * ur;
+    const uint32_t b = n / kSiteBlock, ns = n - b * kSiteBlock;
+    return ((int64_t)(b * ur + r) * kSiteBlock + ns) * um + j;
+}
 
 // Record an error for qcuGetLastStatus()/qcuGetLastError(); returns the status.
 int set_error(int status, const char* fmt, ...);

@@ -443,19 +443,21 @@ __device__ __forceinline__ void f2_sub(float2& a, float2 b) {
 // ---- two RHS per thread (compile-time even m) ----
 // Thread per (half-site, RHS pair j): RHS 2j and 2j+1 sit in one 8-byte word pair of every
 // (spin, colour) row, so each neighbour value is one 8-byte load; the links, their
-// (-W.im, W.re) partners and the neighbour arithmetic serve both RHS.
+// (-W.im, W.re) partners and the neighbour arithmetic serve both RHS.  psi points at the
+// neighbour's row 0 (plus the pair); rs is the distance between rows in 8-byte words
+// (m / 2 in the gathered layout, kSiteBlock m / 2 in the site-blocked one).
 template <int NC, typename S, int MU, int SG, typename LinkFn>
-__device__ __forceinline__ void h16_hop2(float2 (&acc)[2][4][NC], const uint2* __restrict__ psi, int m2,
+__device__ __forceinline__ void h16_hop2(float2 (&acc)[2][4][NC], const uint2* __restrict__ psi, int rs,
                                          LinkFn link) {
     using P = Pk16<S>;
     using T2 = typename P::T2;
     uint32_t h0[2][NC], h1[2][NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-        const uint2 q0 = __ldg(psi + (0 * NC + c) * m2);
-        const uint2 q1 = __ldg(psi + (1 * NC + c) * m2);
-        const uint2 q2 = __ldg(psi + (2 * NC + c) * m2);
-        const uint2 q3 = __ldg(psi + (3 * NC + c) * m2);
+        const uint2 q0 = __ldg(psi + (0 * NC + c) * rs);
+        const uint2 q1 = __ldg(psi + (1 * NC + c) * rs);
+        const uint2 q2 = __ldg(psi + (2 * NC + c) * rs);
+        const uint2 q3 = __ldg(psi + (3 * NC + c) * rs);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const uint32_t p0 = r ? q0.y : q0.x, p1 = r ? q1.y : q1.x;
@@ -541,7 +543,7 @@ __device__ inline void grid_reduce_pairs(const float2 (&v)[2][NV > 0 ? NV : 1], 
     publish_and_finish<NV>(bsum, m, ra);
 }
 
-template <int NC, typename S, bool DAG, int EPI, int MR>
+template <int NC, typename S, bool DAG, int EPI, int MR, bool BLK>
 __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams p) {
     using P = Pk16<S>;
     using S2 = typename St<S>::S2;
@@ -571,8 +573,14 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
 #pragma unroll
         for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[q][k] = make_float2(0.f, 0.f);
     const int64_t site_stride = ((int64_t)gridDim.x * blockDim.x) / M2;
+    // 8-byte word of (site n, row 0, pair 0) and the distance between rows
+    constexpr int64_t RS = BLK ? (int64_t)kSiteBlock * M2 : M2;
+    auto sbase = [](int64_t n) -> int64_t {
+        if constexpr (BLK) return (n / kSiteBlock) * (kNs * NC * kSiteBlock * M2) + (n % kSiteBlock) * M2;
+        else return n * (kNs * NC * M2);
+    };
     for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / M2 + threadIdx.x / M2; site < vh; site += site_stride) {
-        if constexpr (EPI != EPI_PLAIN) {
+        if constexpr (EPI != EPI_PLAIN && !BLK) {
             const int64_t off = (int64_t)j * 32;
             if (off < site_len) {
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.x) + site * site_len + off));
@@ -591,51 +599,50 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
                 for (int cc = 0; cc < NC; ++cc) acc[r][s][cc] = make_float2(0.f, 0.f);
         uint32_t w[N2];
         auto link = [&](int a, int b) { return make_uint2(w[a * NC + b], times_i(w[a * NC + b])); };
-        constexpr int64_t sl2 = site_len / 2;   // uint2 per site
         {
             const int64_t nf = site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh);
             h16_load_link<NC, true>(w, gf + site * N2, 0u);
-            h16_hop2<NC, S, 0, SF>(acc, in2 + nf * sl2, M2, link);
+            h16_hop2<NC, S, 0, SF>(acc, in2 + sbase(nf), RS, link);
             const int64_t nb = site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1));
             h16_load_link<NC, false>(w, gb + nb * N2, 0u);
-            h16_hop2<NC, S, 0, SB>(acc, in2 + nb * sl2, M2, link);
+            h16_hop2<NC, S, 0, SB>(acc, in2 + sbase(nb), RS, link);
         }
         {
             const int64_t nf = site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy);
             h16_load_link<NC, true>(w, gf + gmu + site * N2, 0u);
-            h16_hop2<NC, S, 1, SF>(acc, in2 + nf * sl2, M2, link);
+            h16_hop2<NC, S, 1, SF>(acc, in2 + sbase(nf), RS, link);
             const int64_t nb = site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
             h16_load_link<NC, false>(w, gb + gmu + nb * N2, 0u);
-            h16_hop2<NC, S, 1, SB>(acc, in2 + nb * sl2, M2, link);
+            h16_hop2<NC, S, 1, SB>(acc, in2 + sbase(nb), RS, link);
         }
         {
             const int64_t nf = site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz);
             h16_load_link<NC, true>(w, gf + 2 * gmu + site * N2, 0u);
-            h16_hop2<NC, S, 2, SF>(acc, in2 + nf * sl2, M2, link);
+            h16_hop2<NC, S, 2, SF>(acc, in2 + sbase(nf), RS, link);
             const int64_t nb = site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
             h16_load_link<NC, false>(w, gb + 2 * gmu + nb * N2, 0u);
-            h16_hop2<NC, S, 2, SB>(acc, in2 + nb * sl2, M2, link);
+            h16_hop2<NC, S, 2, SB>(acc, in2 + sbase(nb), RS, link);
         }
         {
             const bool wf = (c.t + 1 == Lt);
             const int64_t nf = site + (wf ? -(int64_t)(Lt - 1) * st : st);
             h16_load_link<NC, true>(w, gf + 3 * gmu + site * N2, wf ? tflip : 0u);
-            h16_hop2<NC, S, 3, SF>(acc, in2 + nf * sl2, M2, link);
+            h16_hop2<NC, S, 3, SF>(acc, in2 + sbase(nf), RS, link);
             const bool wb = (c.t == 0);
             const int64_t nb = site + (wb ? (int64_t)(Lt - 1) * st : -st);
             h16_load_link<NC, false>(w, gb + 3 * gmu + nb * N2, wb ? tflip : 0u);
-            h16_hop2<NC, S, 3, SB>(acc, in2 + nb * sl2, M2, link);
+            h16_hop2<NC, S, 3, SB>(acc, in2 + sbase(nb), RS, link);
         }
         // epilogue: the two RHS of every (spin, colour) row as one 8-byte word pair
         uint2* __restrict__ out2 = reinterpret_cast<uint2*>(p.out);
         const uint2* __restrict__ x2 = reinterpret_cast<const uint2*>(p.x);
         const uint2* __restrict__ r02 = reinterpret_cast<const uint2*>(p.r0);
-        const int64_t base2 = site * sl2 + j;
+        const int64_t base2 = sbase(site) + j;
 #pragma unroll
         for (int s = 0; s < 4; ++s)
 #pragma unroll
             for (int cc = 0; cc < NC; ++cc) {
-                const int64_t o = base2 + (int64_t)(s * NC + cc) * M2;
+                const int64_t o = base2 + (int64_t)(s * NC + cc) * RS;
                 if (EPI == EPI_PLAIN) {
                     const S2 a0 = St<S>::cv(acc[0][s][cc]), a1 = St<S>::cv(acc[1][s][cc]);
                     out2[o] = make_uint2(bits(a0), bits(a1));
@@ -682,18 +689,18 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
     if constexpr (NV > 0) grid_reduce_pairs<NV>(red, MR, p.red);
 }
 
-template <int NC, typename S, int MR>
-int launch16p(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+template <int NC, typename S, int MR, bool BLK>
+int launch16p_l(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
         return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
     void (*k)(const HopParams) = nullptr;
     switch (epi) {
-        case EPI_PLAIN: k = dagger ? hop16p_kernel<NC, S, true, EPI_PLAIN, MR> : hop16p_kernel<NC, S, false, EPI_PLAIN, MR>; break;
-        case EPI_XPAY: k = dagger ? hop16p_kernel<NC, S, true, EPI_XPAY, MR> : hop16p_kernel<NC, S, false, EPI_XPAY, MR>; break;
-        case EPI_SCHUR_R0: k = hop16p_kernel<NC, S, false, EPI_SCHUR_R0, MR>; break;
-        case EPI_SCHUR_TS: k = hop16p_kernel<NC, S, false, EPI_SCHUR_TS, MR>; break;
-        case EPI_SCHUR: k = hop16p_kernel<NC, S, false, EPI_SCHUR, MR>; break;
-        case EPI_RESID: k = hop16p_kernel<NC, S, false, EPI_RESID, MR>; break;
+        case EPI_PLAIN: k = dagger ? hop16p_kernel<NC, S, true, EPI_PLAIN, MR, BLK> : hop16p_kernel<NC, S, false, EPI_PLAIN, MR, BLK>; break;
+        case EPI_XPAY: k = dagger ? hop16p_kernel<NC, S, true, EPI_XPAY, MR, BLK> : hop16p_kernel<NC, S, false, EPI_XPAY, MR, BLK>; break;
+        case EPI_SCHUR_R0: k = hop16p_kernel<NC, S, false, EPI_SCHUR_R0, MR, BLK>; break;
+        case EPI_SCHUR_TS: k = hop16p_kernel<NC, S, false, EPI_SCHUR_TS, MR, BLK>; break;
+        case EPI_SCHUR: k = hop16p_kernel<NC, S, false, EPI_SCHUR, MR, BLK>; break;
+        case EPI_RESID: k = hop16p_kernel<NC, S, false, EPI_RESID, MR, BLK>; break;
         default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
     }
     constexpr int M2 = MR / 2;
@@ -703,6 +710,11 @@ int launch16p(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     k<<<grid, block, 0, st>>>(p);
     QCUB_CHECK_LAUNCH();
     return QCU_SUCCESS;
+}
+
+template <int NC, typename S, int MR>
+int launch16p(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    return p.blocked ? launch16p_l<NC, S, MR, true>(p, dagger, epi, st) : launch16p_l<NC, S, MR, false>(p, dagger, epi, st);
 }
 
 // RHS counts with a compile-time specialisation (SU(3) only; other shapes use runtime m)
@@ -756,9 +768,15 @@ bool hop16_pairs_supported(int nc, int m, int prec) {
     return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc == 3 && (m == 8 || m == 12 || m == 16);
 }
 
+bool hop16_blocked_supported(int nc, int m, int prec, int64_t vh) {
+    return hop16_pairs_supported(nc, m, prec) && vh % kSiteBlock == 0 && vh * 4 * nc * m < ((int64_t)1 << 31);
+}
+
 int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
     if (!hop16_pairs_supported(nc, p.m, prec))
         return set_error(QCU_ERR_UNSUPPORTED, "two-RHS packed hop: n_color %d, m %d", nc, p.m);
+    if (p.blocked && !hop16_blocked_supported(nc, p.m, prec, p.g.vh))
+        return set_error(QCU_ERR_UNSUPPORTED, "site-blocked layout: half volume %lld", (long long)p.g.vh);
     if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");
     auto go = [&](auto tag) -> int {
         using S = decltype(tag);

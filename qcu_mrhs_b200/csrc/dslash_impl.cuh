@@ -46,6 +46,7 @@ struct HopParams {
     RedArgs red;
     const int* done;   // if non-null and *done != 0 the kernel returns at once
     const int* gate;   // if non-null and *gate == 0 the kernel returns at once
+    int blocked;       // 1: in, out, x and r0 in the site-blocked layout (kSiteBlock)
 };
 
 __device__ __forceinline__ bool skip_launch(const int* done, const int* gate) {

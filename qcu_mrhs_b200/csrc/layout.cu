@@ -220,6 +220,38 @@ int gauge_reorder(void* dst, const void* src, const int L[4], int nc, int prec, 
     return site_reorder(dst, src, L, nc * nc, 4, prec, to_eo, st);
 }
 
+// gathered [Vh][4N][m] <-> site-blocked (kSiteBlock) multi-RHS half-lattice field
+template <typename S>
+__global__ void site_block_kernel(typename St<S>::S2* __restrict__ dst, const typename St<S>::S2* __restrict__ src,
+                                  int64_t n, int m, int rows, int to_blocked) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = site_blocked_index(i, m, rows);
+        if (to_blocked) dst[b] = src[i];
+        else dst[i] = src[b];
+    }
+}
+
+int site_block_reorder(void* dst, const void* src, int64_t vh, int nc, int m, int prec, int to_blocked,
+                       cudaStream_t st) {
+    if (!dst || !src) return set_error(QCU_ERR_INVALID, "null pointer");
+    if (dst == src) return set_error(QCU_ERR_INVALID, "the site-blocked reorder cannot run in place");
+    if (nc < 1 || nc > kMaxColor || m < 1 || m > kMaxRhs)
+        return set_error(QCU_ERR_INVALID, "n_color=%d m_rhs=%d", nc, m);
+    if (vh < 1 || vh % kSiteBlock)
+        return set_error(QCU_ERR_INVALID, "half volume %lld is not a multiple of %d", (long long)vh, kSiteBlock);
+    const int64_t n = vh * 4 * nc * m;
+    if (n >= ((int64_t)1 << 31)) return set_error(QCU_ERR_UNSUPPORTED, "site-blocked field beyond 2^31 complex");
+    return dispatch_prec(prec, [&](auto tag) -> int {
+        using S = decltype(tag);
+        auto k = site_block_kernel<S>;
+        const int grid = resident_grid(k, kLayoutThreads, n);
+        k<<<grid, kLayoutThreads, 0, st>>>(static_cast<typename St<S>::S2*>(dst),
+                                           static_cast<const typename St<S>::S2*>(src), n, m, 4 * nc, to_blocked);
+        QCUB_CHECK_LAUNCH();
+        return QCU_SUCCESS;
+    });
+}
+
 int fermion_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo, cudaStream_t st) {
     return site_reorder(dst, src, L, 4 * nc, 1, prec, to_eo, st);
 }

@@ -16,5 +16,8 @@ int gauge_reorder(void* dst, const void* src, const int L[4], int nc, int prec, 
                   cudaStream_t st);
 // fermion [Lt][Lz][Ly][Lx][4][nc] <-> [2][Vh][4][nc]
 int fermion_reorder(void* dst, const void* src, const int L[4], int nc, int prec, int to_eo, cudaStream_t st);
+// multi-RHS half-lattice field: gathered [Vh][4nc][m] <-> site-blocked (kSiteBlock)
+int site_block_reorder(void* dst, const void* src, int64_t vh, int nc, int m, int prec, int to_blocked,
+                       cudaStream_t st);
 
 }  // namespace qcub

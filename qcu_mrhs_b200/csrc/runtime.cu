@@ -150,6 +150,7 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (p.g.L[0] % 2 || p.g.L[0] < 2 || p.g.L[1] < 1 || p.g.L[2] < 1 || p.g.L[3] < 1)
         return set_error(QCU_ERR_INVALID, "lattice %dx%dx%dx%d (Lx must be even)", p.g.L[0], p.g.L[1],
                          p.g.L[2], p.g.L[3]);
+    if (p.blocked) return hop16_pairs_launch(p, nc, prec, dagger, epi, st);
     int kind = g_hop_kind;
     if (kind == QCU_HOP_AUTO) kind = auto_hop_kind(nc, p.m, prec);
     if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec) &&

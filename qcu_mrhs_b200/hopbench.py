@@ -15,7 +15,10 @@ import ctypes
 import json
 
 PRECS = {"f64": 2, "f32": 1, "f16": 0, "bf16": 4}
-KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"]
+KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs",
+           "packed16_pairs_blocked"]
+# the last entry is the two-RHS kernel on the site-blocked layout (qcuDslashMrhsSiteBlocked)
+BLOCKED = KERNELS.index("packed16_pairs_blocked")
 
 
 def hop_bytes(vh, nc, m, s):
@@ -41,17 +44,18 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
     st = torch.cuda.current_stream()
     sp = ctypes.c_void_p(st.cuda_stream)
     lib = q.lib()
-    q.check(lib.qcuSetHopKernel(kernel))
+    q.check(lib.qcuSetHopKernel(q.HOP_PACKED16_PAIRS if kernel == BLOCKED else kernel))
+    hop = lib.qcuDslashMrhsSiteBlocked if kernel == BLOCKED else lib.qcuDslashMrhs
     bufs = (a, b)
     for i in range(warmup):
-        q.check(lib.qcuDslashMrhs(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
-                                  i & 1, 0, t_sign, prec, sp))
+        q.check(hop(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
+                    i & 1, 0, t_sign, prec, sp))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(st)
     for i in range(reps):
-        q.check(lib.qcuDslashMrhs(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
-                                  i & 1, 0, t_sign, prec, sp))
+        q.check(hop(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
+                    i & 1, 0, t_sign, prec, sp))
     e1.record(st)
     torch.cuda.synchronize()
     dur = e0.elapsed_time(e1) / 1e3 / reps

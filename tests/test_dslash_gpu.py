@@ -211,3 +211,78 @@ def test_hop_rejects_bad_arguments():
     assert q.lib().qcuDslashMrhs(p, p, p, L, 3, 4, 2, 0, 1.0, q.DOUBLE, None) == q.ERR_INVALID
     assert q.lib().qcuDslashMrhs(p, p, p, q.lattice((7, 8, 8, 8)), 3, 4, 0, 0, 1.0, q.DOUBLE, None) == q.ERR_INVALID
     assert q.lib().qcuDslashMrhs(p, p, p, L, 3, 4, 0, 0, 1.0, q.UNDEFINED, None) == q.ERR_INVALID
+
+
+def _blocked_ref(a, m, nc):
+    """numpy statement of the site-blocked layout: [Vh][4N][m] -> [Vh/32][4N][32][m]."""
+    vh = a.shape[0]
+    return a.reshape(vh // 32, 32, 4 * nc, m).transpose(0, 2, 1, 3).copy()
+
+
+@pytest.mark.parametrize("prec", [q.DOUBLE, q.HALF, q.BF16])
+@pytest.mark.parametrize("nc,m", [(3, 12), (2, 5), (3, 8)])
+def test_site_blocked_reorder(prec, nc, m):
+    """Gathered -> site-blocked is the stated permutation and comes back exactly."""
+    L = (8, 8, 4, 4)
+    vh = F.half_volume(L)
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal((vh, 4, nc, m)) + 1j * rng.standard_normal((vh, 4, nc, m))
+    da = to_dev(a, prec)
+    db = empty_dev(a.shape, prec)
+    q.check(q.lib().qcuSiteBlockMrhs(db.data_ptr(), da.data_ptr(), vh, nc, m, prec, 1, None))
+    sync()
+    got = from_dev(db).reshape(vh // 32, 4 * nc, 32, m)
+    assert np.array_equal(got, _blocked_ref(from_dev(da).reshape(vh, 4 * nc, m), m, nc))
+    back = empty_dev(a.shape, prec)
+    q.check(q.lib().qcuSiteBlockMrhs(back.data_ptr(), db.data_ptr(), vh, nc, m, prec, 0, None))
+    sync()
+    assert np.array_equal(from_dev(back), from_dev(da))
+    assert q.lib().qcuSiteBlockMrhs(db.data_ptr(), da.data_ptr(), vh - 1, nc, m, prec, 1, None) == q.ERR_INVALID
+    assert q.lib().qcuSiteBlockMrhs(da.data_ptr(), da.data_ptr(), vh, nc, m, prec, 1, None) == q.ERR_INVALID
+
+
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16])
+@pytest.mark.parametrize("m", [8, 12, 16])
+@pytest.mark.parametrize("dagger", [0, 1])
+def test_site_blocked_hop_matches_gathered(oracle_lib, prec, m, dagger):
+    """The two-RHS packed kernel on site-blocked fields gives bit for bit the output of the
+    same kernel on the gathered layout (same arithmetic, other addresses), both parities,
+    antiperiodic t; and it is within the 16-bit tolerance of the oracle."""
+    L, nc = (8, 4, 4, 8), 3
+    vh = F.half_volume(L)
+    gauge, inp = _problem(L, nc, m, 61)
+    d_in, d_g = to_dev(inp, prec), to_dev(gauge, prec)
+    d_bin = empty_dev(inp.shape, prec)
+    q.check(q.lib().qcuSiteBlockMrhs(d_bin.data_ptr(), d_in.data_ptr(), vh, nc, m, prec, 1, None))
+    q.check(q.lib().qcuSetHopKernel(q.HOP_PACKED16_PAIRS))
+    try:
+        for parity in (0, 1):
+            d_out = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuDslashMrhs(d_out.data_ptr(), d_in.data_ptr(), d_g.data_ptr(), q.lattice(L), nc, m,
+                                          parity, dagger, -1.0, prec, None))
+            d_bout = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuDslashMrhsSiteBlocked(d_bout.data_ptr(), d_bin.data_ptr(), d_g.data_ptr(),
+                                                     q.lattice(L), nc, m, parity, dagger, -1.0, prec, None))
+            d_back = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuSiteBlockMrhs(d_back.data_ptr(), d_bout.data_ptr(), vh, nc, m, prec, 0, None))
+            sync()
+            import torch
+            assert torch.equal(d_back, d_out)
+            ref = oracle_lib.hop(_round(inp, prec), _round(gauge, prec), L, parity, bool(dagger), -1.0)
+            assert rel_err(from_dev(d_back), ref) <= TOL[prec]
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
+
+
+def test_site_blocked_hop_rejects_unsupported_shapes():
+    L, nc, m = (8, 4, 4, 8), 3, 12
+    vh = F.half_volume(L)
+    a = empty_dev((vh, 4, nc, m), q.HALF)
+    g = empty_dev((4, 2, vh, nc, nc), q.HALF)
+    lat = q.lattice(L)
+    assert q.lib().qcuDslashMrhsSiteBlocked(a.data_ptr(), a.data_ptr(), g.data_ptr(), lat, nc, 4, 0, 0, 1.0,
+                                            q.HALF, None) == q.ERR_UNSUPPORTED
+    assert q.lib().qcuDslashMrhsSiteBlocked(a.data_ptr(), a.data_ptr(), g.data_ptr(), lat, nc, m, 0, 0, 1.0,
+                                            q.DOUBLE, None) == q.ERR_UNSUPPORTED
+    assert q.lib().qcuDslashMrhsSiteBlocked(a.data_ptr(), a.data_ptr(), g.data_ptr(), q.lattice((6, 2, 2, 2)),
+                                            nc, m, 0, 0, 1.0, q.HALF, None) == q.ERR_UNSUPPORTED
