@@ -47,7 +47,10 @@ const char *qcuGetLastError(void);
 /* ---- solver selection for qcuInvert ---- */
 #define QCU_SOLVER_REFERENCE 0 /* reference policy-1 BiCGStab, output precision, recursive residual */
 #define QCU_SOLVER_FUSED 1     /* same iteration, fused device-resident kernels, CUDA graph */
-#define QCU_SOLVER_MIXED 2     /* sloppy-precision inner BiCGStab with FP64 reliable updates */
+#define QCU_SOLVER_MIXED 2     /* sloppy-precision inner BiCGStab with FP64 reliable updates; a
+                                  sloppy breakdown restarts from the FP64 residual, and an FP64
+                                  residual that stops falling (no 2% gain over 32 reliable
+                                  updates) ends the solve with QCU_ERR_NOT_CONVERGED */
 #define QCU_SOLVER_PRECOND 3   /* FP64 BiCGStab on the full system, right-preconditioned by the
                                   learned preconditioner of qcuSetPreconditioner; falls back to
                                   QCU_SOLVER_FUSED if it does not converge */

@@ -4,6 +4,7 @@
 // context's own stream; each qcu.h entry point synchronises before returning, as the
 // reference does (src/qcu_interface.cu:131,168,359).
 #include <mutex>
+#include <string>
 
 #include "../../include/qcu.h"
 #include "blas.h"
@@ -313,12 +314,13 @@ static int invert_impl(int max_iter, double tol) {
     else
         rc = mixed ? solve_mixed(c, x, b, max_iter, tol) : solve_fused(c, x, b, max_iter, tol);
     const int solve_rc = rc;
+    const std::string solve_msg = last_message();   // a copy: set_error below rewrites the buffer
     if (rc != QCU_SUCCESS && rc != QCU_ERR_NOT_CONVERGED && rc != QCU_ERR_BREAKDOWN) return rc;
     // write the solution (also the last iterate when not converged)
     for (int par = 0; par < 2; ++par)
         if ((rc = scatter_mrhs(outs[par], P, x + par * hb, P, c.g.vh, c.nc, c.m, c.stream))) return rc;
     QCUB_CUDA_CHECK(cudaStreamSynchronize(c.stream));
-    if (solve_rc != QCU_SUCCESS) return set_error(solve_rc, "%s", last_message());
+    if (solve_rc != QCU_SUCCESS) return set_error(solve_rc, "%s", solve_msg.c_str());
     return QCU_SUCCESS;
 }
 

@@ -208,7 +208,9 @@ bicg_p_kernel(typename St<S>::S2* __restrict__ p, const typename St<S>::S2* __re
 
 __device__ __forceinline__ bool mp_skip(const BicgScalars* sc) { return sc->done || !sc->gate; }
 
-// x64 += e / scale_j ; e = 0     (gated by a pending reliable update)
+// x64 += e / scale_j ; e = 0     (gated by a pending reliable update).  Non-finite elements
+// of e (a sloppy iterate that overflowed before the breakdown was caught) are dropped, so
+// x64 stays finite and the restart continues from it.
 static __global__ void __launch_bounds__(kRedThreads)
 mp_accum_kernel(double2* __restrict__ x64, float2* __restrict__ e, const BicgScalars* __restrict__ sc,
                 int64_t n, int m) {
@@ -217,10 +219,12 @@ mp_accum_kernel(double2* __restrict__ x64, float2* __restrict__ e, const BicgSca
     const double inv = 1.0 / sc->scale[j];
     QCUB_GRID_LOOP(gi, n) {
         const float2 ev = e[gi];
-        double2 xv = x64[gi];
-        xv.x += inv * ev.x;
-        xv.y += inv * ev.y;
-        x64[gi] = xv;
+        if (isfinite(ev.x) && isfinite(ev.y)) {
+            double2 xv = x64[gi];
+            xv.x += inv * ev.x;
+            xv.y += inv * ev.y;
+            x64[gi] = xv;
+        }
         e[gi] = make_float2(0.f, 0.f);
     }
 }
@@ -265,13 +269,24 @@ mp_load_kernel(typename St<S>::S2* __restrict__ rs, typename St<S>::S2* __restri
 // init: first call (sets scale from ||r64|| without touching counters).
 static __global__ void mp_update_kernel(BicgScalars* sc, int m, int init) {
     if (!init && mp_skip(sc)) return;
-    __shared__ int all_conv;
-    if (threadIdx.x == 0) all_conv = 1;
+    __shared__ int all_conv, stalled;
+    if (threadIdx.x == 0) { all_conv = 1; stalled = 0; }
     __syncthreads();
     const int j = threadIdx.x;
     if (j < m) {
         const double r2 = sc->rtrue2[j];
         const bool conv = r2 <= sc->tol2 * sc->bfull2[j];
+        if (init) {
+            sc->best2[j] = r2;
+            sc->stall[j] = 0;
+        } else if (sc->active[j] && !conv) {
+            if (r2 < 0.98 * sc->best2[j]) {
+                sc->best2[j] = r2;
+                sc->stall[j] = 0;
+            } else if (++sc->stall[j] >= kStallUpdates) {
+                atomicOr(&stalled, 1);
+            }
+        }
         if (conv) sc->active[j] = 0;
         if (!conv) atomicAnd(&all_conv, 0);
         // scale so that the sloppy residual has unit RMS element (O(1) values keep FP16
@@ -290,6 +305,9 @@ static __global__ void mp_update_kernel(BicgScalars* sc, int m, int init) {
         if (!init) sc->reliable += 1;
         if (all_conv) {
             sc->status = 1;
+            sc->done = 1;
+        } else if (stalled) {
+            sc->status = 4;
             sc->done = 1;
         }
     }

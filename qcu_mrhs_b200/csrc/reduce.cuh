@@ -45,7 +45,19 @@ struct BicgScalars {
     double maxr[kMaxRhs];               // max sloppy ||r_j|| since the last update
     double bfull2[kMaxRhs];             // ||b_j||^2 of the full system (stopping reference)
     double rtrue2[kMaxRhs];             // ||b' - A x||^2 at the last reliable update
+    double beta_max;                    // |beta| above it counts as a sloppy breakdown
+    double best2[kMaxRhs];              // smallest rtrue2 so far (stagnation guard)
+    int stall[kMaxRhs];                 // reliable updates since rtrue2 last fell below 0.98 best2
 };
+
+// Mixed solver guards.  With FP16 storage a sloppy |beta| above kMaxHalfBeta (omega near
+// zero) counts as a breakdown: p = r + beta (p - omega v) would leave the FP16 range, so
+// the pending reliable update restarts p and r0 from the FP64 residual instead (BF16 and
+// FP32 share the FP32 exponent range and take no such bound).  The solve stops as not
+// converged (status 4) once an unconverged RHS's FP64 residual has not fallen by 2% over
+// kStallUpdates reliable updates in a row.
+constexpr double kMaxHalfBeta = 1e3;
+constexpr int kStallUpdates = 32;
 
 enum Finisher : int {
     FIN_NONE = 0,     // only publish the sums into sc->red (or the result array)
@@ -136,7 +148,11 @@ __device__ inline void run_finisher(const RedArgs& ra, int m, const double2* sum
                             s_flags[0] = 0;   // reused below as "update needed" (inverted)
                         b = cdiv(cmul(sc->alpha[j], rho_new), sc->omega[j]);
                         b = cdiv(b, sc->rho[j]);
-                        if (!cfinite(b)) { s_flags[1] = 1; b = make_double2(0.0, 0.0); }
+                        if (!cfinite(b) || !(b.x * b.x + b.y * b.y <= sc->beta_max * sc->beta_max) ||
+                            !isfinite(rn2)) {
+                            s_flags[1] = 1;
+                            b = make_double2(0.0, 0.0);
+                        }
                         sc->rho[j] = rho_new;
                     }
                     sc->beta[j] = b;

@@ -13,7 +13,10 @@
 //   BF16 storage, FP32 arithmetic, FP64 reductions), solution increments accumulated in
 //   FP32, and reliable updates in FP64: x += e, r = b' - A x recomputed in FP64 whenever
 //   the sloppy residual has fallen by `reliable_delta` or claims convergence; the solve
-//   stops only on the FP64 true residual.
+//   stops only on the FP64 true residual.  A sloppy breakdown (non-finite or huge beta,
+//   non-finite residual) restarts p and r0 from the FP64 residual at the next reliable
+//   update; non-finite increments never reach x; and a FP64 residual that stops falling
+//   ends the solve as not converged instead of running to max_iteration.
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -97,6 +100,7 @@ int prepare_scalars(Context& c, BicgScalars* dsc, int max_iter, double tol, int 
     h.max_iter = max_iter;
     h.mixed = mixed;
     h.delta = c.opts.reliable_delta > 0 ? c.opts.reliable_delta : 0.1;
+    h.beta_max = mixed && c.opts.sloppy_precision == QCU_PRECISION_HALF ? kMaxHalfBeta : 1e300;
     h.len_per_rhs = (double)c.half_len();
     for (int j = 0; j < c.m; ++j) {
         h.active[j] = 1;
@@ -333,7 +337,9 @@ int SchurSolve::end() {
     if (c.stats.status != QCU_SUCCESS)
         return set_error(c.stats.status, "%sBiCGStab stopped after %d iterations (%s)", mixed_ ? "mixed " : "",
                          c.stats.iterations,
-                         c.stats.status == QCU_ERR_BREAKDOWN ? "breakdown" : "max_iteration reached");
+                         c.stats.status == QCU_ERR_BREAKDOWN ? "breakdown"
+                         : c.host_sc->status == 4           ? "the FP64 residual stagnated"
+                                                            : "max_iteration reached");
     return QCU_SUCCESS;
 }
 

@@ -87,6 +87,9 @@ def test_mat_qcu_half_precision_dslash(oracle_lib):
     assert rel_err(got, oracle_lib.mat(psi, gauge, L, kappa)) <= 3e-3
 
 
+_LAST = {"error": ""}
+
+
 def _invert(L, nc, m, kappa, tol, seed, opts=None, max_iter=2000, kind="haar", t_boundary=1.0):
     gauge, dg = _setup(L, nc, m, kappa, seed, kind=kind)
     o = q.default_options()
@@ -103,6 +106,7 @@ def _invert(L, nc, m, kappa, tol, seed, opts=None, max_iter=2000, kind="haar", t
         q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
     q.lib().qcuInvert(max_iter, tol)
     st = q.status()
+    _LAST["error"] = q.last_error()   # reading the statistics clears the message
     x = np.stack([from_dev(o) for o in outs])
     return gauge, b, x, st, q.solve_stats()
 
@@ -228,6 +232,25 @@ def test_cgnr_not_converged_and_options():
     o.solver = q.SOLVER_CGNR
     init(L, nc, m, q.HALF, q.HALF)
     assert q.lib().qcuSetSolverOptions(ctypes.byref(o)) == q.SUCCESS
+
+
+@pytest.mark.parametrize("sloppy", [q.SINGLE, q.HALF])
+def test_mixed_precision_stops_when_the_residual_stagnates(oracle_lib, sloppy):
+    """A tolerance below FP64 reach: the FP64 residual stops falling, and the mixed solver
+    ends as not converged after the stall limit (32 reliable updates without a 2% gain)
+    instead of iterating to max_iteration; x is finite and as good as FP64 allows."""
+    L, nc, m, kappa = (8, 8, 8, 8), 3, 4, 0.12
+    gauge, b, x, st, stats = _invert(L, nc, m, kappa, 1e-17, 17, max_iter=5000, kind="smooth",
+                                     t_boundary=-1.0,
+                                     opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy,
+                                           "reliable_delta": 0.1})
+    assert st == q.ERR_NOT_CONVERGED
+    assert "stagnated" in _LAST["error"]
+    assert stats.iterations < 5000
+    assert stats.reliable_updates >= 32
+    res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+    true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+    assert np.all(np.isfinite(x)) and np.all(true_rel <= 1e-13)
 
 
 def test_invert_not_converged_status():
