@@ -165,7 +165,7 @@ int bicg_step(int step, int prec, int x_prec, const BicgStepArgs& a, cudaStream_
 int mp_accum(void* x64, void* e, BicgScalars* sc, int64_t len, int m, cudaStream_t st) {
     const int block = rhs_block(m);
     const int grid = resident_grid(mp_accum_kernel, block, len * m);
-    mp_accum_kernel<<<grid, block, 0, st>>>(static_cast<double2*>(x64), static_cast<float2*>(e), sc,
+    mp_accum_kernel<<<grid, block, 0, st>>>(static_cast<double2*>(x64), static_cast<const float2*>(e), sc,
                                             len * m, m);
     QCUB_CHECK_LAUNCH();
     return QCU_SUCCESS;

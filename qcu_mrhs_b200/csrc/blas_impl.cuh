@@ -145,7 +145,8 @@ bicg_s_kernel(typename St<S>::S2* __restrict__ s, const typename St<S>::S2* __re
     }
 }
 
-// x += alpha p + omega s ; r = s - omega t ; reduce |r|^2, <r0, r>  (FIN_BETA)
+// x += alpha p + omega s ; r = s - omega t ; reduce |r|^2, <r0, r>  (FIN_BETA).
+// With sc->x_fresh (mixed solver, first step after a reliable update) x = alpha p + omega s.
 template <typename S, typename SX>
 __global__ void __launch_bounds__(kRedThreads)
 bicg_xr_kernel(typename St<SX>::S2* __restrict__ x, typename St<S>::S2* __restrict__ r,
@@ -161,11 +162,12 @@ bicg_xr_kernel(typename St<SX>::S2* __restrict__ x, typename St<S>::S2* __restri
     const A2 omA = from_d2<A2>(sc->omega[j]);
     using R = typename RedAcc<S>::T;
     R v[2][2] = {{0, 0}, {0, 0}};
+    const bool fresh = sc->x_fresh != 0;
     QCUB_GRID_LOOP(gi, n) {
         const A2 pv = St<S>::ld(p[gi]);
         const A2 sv = St<S>::ld(s[gi]);
         const A2 tv = St<S>::ld(t[gi]);
-        X2 xv = St<SX>::ld(x[gi]);
+        X2 xv = fresh ? mk2<X2>(0, 0) : St<SX>::ld(x[gi]);
         const X2 ap = cmulA(al, mk2<X2>(pv.x, pv.y));
         const X2 os = cmulA(om, mk2<X2>(sv.x, sv.y));
         xv.x += ap.x + os.x;
@@ -183,14 +185,15 @@ bicg_xr_kernel(typename St<SX>::S2* __restrict__ x, typename St<S>::S2* __restri
     reduce_partials<R, 2>(v, m, ra);
 }
 
-// p = r + beta (p - omega v)
+// p = r + beta (p - omega v); clears x_fresh (the STEP_XR before it has read it)
 template <typename S>
 __global__ void __launch_bounds__(kRedThreads)
 bicg_p_kernel(typename St<S>::S2* __restrict__ p, const typename St<S>::S2* __restrict__ r,
-              const typename St<S>::S2* __restrict__ v, const BicgScalars* __restrict__ sc, int64_t n,
+              const typename St<S>::S2* __restrict__ v, BicgScalars* __restrict__ sc, int64_t n,
               int m) {
     using A2 = typename St<S>::A2;
     if (sc->done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->x_fresh = 0;
     const int j = threadIdx.x % m;
     const A2 be = from_d2<A2>(sc->beta[j]);
     const A2 om = from_d2<A2>(sc->omega[j]);
@@ -208,13 +211,15 @@ bicg_p_kernel(typename St<S>::S2* __restrict__ p, const typename St<S>::S2* __re
 
 __device__ __forceinline__ bool mp_skip(const BicgScalars* sc) { return sc->done || !sc->gate; }
 
-// x64 += e / scale_j ; e = 0     (gated by a pending reliable update).  Non-finite elements
-// of e (a sloppy iterate that overflowed before the breakdown was caught) are dropped, so
-// x64 stays finite and the restart continues from it.
+// x64 += e / scale_j (gated by a pending reliable update); e is not zeroed: x_fresh makes
+// the next STEP_XR overwrite it.  Non-finite elements of e (a sloppy iterate that overflowed
+// before the breakdown was caught) are dropped, so x64 stays finite and the restart
+// continues from it.
 static __global__ void __launch_bounds__(kRedThreads)
-mp_accum_kernel(double2* __restrict__ x64, float2* __restrict__ e, const BicgScalars* __restrict__ sc,
+mp_accum_kernel(double2* __restrict__ x64, const float2* __restrict__ e, BicgScalars* __restrict__ sc,
                 int64_t n, int m) {
     if (mp_skip(sc)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->x_fresh = 1;
     const int j = threadIdx.x % m;
     const double inv = 1.0 / sc->scale[j];
     QCUB_GRID_LOOP(gi, n) {
@@ -225,7 +230,6 @@ mp_accum_kernel(double2* __restrict__ x64, float2* __restrict__ e, const BicgSca
             xv.y += inv * ev.y;
             x64[gi] = xv;
         }
-        e[gi] = make_float2(0.f, 0.f);
     }
 }
 

@@ -38,6 +38,8 @@ struct BicgScalars {
     int gate;                           // 1: a reliable update is pending
     int reliable;                       // reliable updates done
     int restart;                        // 1: the pending update also resets p and r0 (breakdown)
+    int x_fresh;                        // 1: the next STEP_XR writes the FP32 increment instead of
+                                        //    adding to it (it was just folded into the FP64 x)
     double delta;                       // update when ||r_j|| < delta * maxr_j
     double len_per_rhs;                 // complex elements per RHS of the sloppy vectors
     double scale[kMaxRhs];              // sloppy vectors hold scale_j * (FP64 quantity)

@@ -99,6 +99,7 @@ int prepare_scalars(Context& c, BicgScalars* dsc, int max_iter, double tol, int 
     h.freeze = c.opts.freeze_converged ? 1 : 0;
     h.max_iter = max_iter;
     h.mixed = mixed;
+    h.x_fresh = mixed;   // the sloppy increment starts from zero
     h.delta = c.opts.reliable_delta > 0 ? c.opts.reliable_delta : 0.1;
     h.beta_max = mixed && c.opts.sloppy_precision == QCU_PRECISION_HALF ? kMaxHalfBeta : 1e300;
     h.len_per_rhs = (double)c.half_len();
@@ -159,8 +160,11 @@ __global__ void cg_beta_kernel(double2* beta, double2* rr, const double2* rr_new
     rr[j] = rr_new[j];
 }
 
+// recompute: the FP64 true residual from x (two hops); else (mixed solver) the FP64 residual
+// of the last reliable update, which is the residual of the returned x up to the rounding
+// of x_e = b_e + kappa D_eo x_o.
 int finish_stats(Context& c, int prec, const void* gauge, const void* x, const void* b, void* tmp,
-                 double2* slots) {
+                 double2* slots, bool recompute = true) {
     QcuSolveStats& st = c.stats;
     st.m_rhs = c.m;
     st.iterations = c.host_sc->iter;
@@ -170,6 +174,13 @@ int finish_stats(Context& c, int prec, const void* gauge, const void* x, const v
     for (int j = 0; j < c.m; ++j) {
         const double b2 = c.host_sc->bnorm2[j];
         st.recursive_residual[j] = b2 > 0 ? std::sqrt(c.host_sc->rnorm2[j] / b2) : 0.0;
+    }
+    if (!recompute) {
+        for (int j = 0; j < c.m; ++j) {
+            const double b2 = c.host_sc->bfull2[j];
+            st.true_residual[j] = b2 > 0 ? std::sqrt(c.host_sc->rtrue2[j] / b2) : std::sqrt(c.host_sc->rtrue2[j]);
+        }
+        return QCU_SUCCESS;
     }
     return true_residual(c, prec, gauge, x, b, tmp, slots, st.true_residual);
 }
@@ -258,9 +269,8 @@ int SchurSolve::begin_mixed(int max_iter, double tol) {
     if ((rc = mrhs_dotc(slots_ + 5 * kMaxRhs, bo, bo, len, c.m, P_, c.ws, c.stream))) return rc;
     set_bfull_kernel<<<1, 64, 0, c.stream>>>(dsc_, slots_ + 4 * kMaxRhs, slots_ + 5 * kMaxRhs, c.m, 1);
     QCUB_CHECK_LAUNCH();
-    // x_o = 0, r64 = b', e = 0, rtrue2 = ||b'||^2
+    // x_o = 0, r64 = b', rtrue2 = ||b'||^2 (the increment e starts from zero through x_fresh)
     QCUB_CUDA_CHECK(cudaMemsetAsync(xo, 0, hb, c.stream));
-    QCUB_CUDA_CHECK(cudaMemsetAsync(v_[10], 0, he, c.stream));
     QCUB_CUDA_CHECK(cudaMemcpyAsync(r64, bp, hb, cudaMemcpyDeviceToDevice, c.stream));
     if ((rc = mrhs_norm(nullptr, r64, len, c.m, P_, c.ws, c.stream, FIN_RNORM, dsc_))) return rc;
     if ((rc = mp_update(dsc_, c.m, 1, c.stream))) return rc;
@@ -325,13 +335,14 @@ int SchurSolve::end() {
     // x_e = b_e + kappa D_eo x_o
     if ((rc = hop.launch(x_, x_ + hb, 0, EPI_XPAY, b_, nullptr, c.kappa))) return rc;
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev1, c.stream));
-    if ((rc = finish_stats(c, P_, g_, x_, b_, tmp, slots_))) return rc;
+    if ((rc = finish_stats(c, P_, g_, x_, b_, tmp, slots_, !mixed_))) return rc;
     if (mixed_)
         for (int j = 0; j < c.m; ++j) {
             const double b2 = c.host_sc->bfull2[j];
             c.stats.recursive_residual[j] = b2 > 0 ? std::sqrt(c.host_sc->rtrue2[j] / b2) : 0.0;
         }
     float ms = 0.f;
+    QCUB_CUDA_CHECK(cudaEventSynchronize(c.ev1));
     QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.solve_seconds = ms * 1e-3;
     if (c.stats.status != QCU_SUCCESS)
@@ -477,6 +488,7 @@ int solve_cgnr(Context& c, void* x, const void* b, int max_iter, double tol) {
     }
     if ((rc = finish_stats(c, P, g, x, b, tmp, sl))) return rc;
     float ms = 0.f;
+    QCUB_CUDA_CHECK(cudaEventSynchronize(c.ev1));
     QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.solve_seconds = ms * 1e-3;
     if (c.stats.status != QCU_SUCCESS)
@@ -553,6 +565,7 @@ int solve_precond(Context& c, Precond* P, void* x, const void* b, int max_iter, 
     QCUB_CUDA_CHECK(cudaEventRecord(c.ev1, c.stream));
     if ((rc = finish_stats(c, D, g64, x, b, v, slots))) return rc;
     float ms = 0.f;
+    QCUB_CUDA_CHECK(cudaEventSynchronize(c.ev1));
     QCUB_CUDA_CHECK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.solve_seconds = ms * 1e-3;
     c.stats.precond_iterations = c.stats.iterations;
