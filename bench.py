@@ -377,7 +377,8 @@ def main():
     h_src = [torch.empty(d_src[0].shape, dtype=torch.float64, pin_memory=True) for _ in range(M)]
     for j in range(M):
         h_src[j].copy_(d_src[j])
-    h_x = [torch.empty_like(h_src[0]) for _ in range(M)]
+    # pinned as well (empty_like does not carry pinning): the solution read-back is a DMA
+    h_x = [torch.empty(d_src[0].shape, dtype=torch.float64, pin_memory=True) for _ in range(M)]
     set_opts(q.SOLVER_MIXED, q.HALF)
     barrier()
     ev0.record()
