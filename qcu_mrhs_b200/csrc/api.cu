@@ -110,6 +110,7 @@ int context_init(Context* c, const int L[4], int n_color, int m_rhs, int in_prec
         cudaGetLastError();
         rc = set_error(QCU_ERR_ALLOC, "pinned host allocation failed");
     }
+    if (!rc) rc = hop16_pairs_prepare();   // before any solve is captured into a graph
     return rc;
 }
 

@@ -15,6 +15,8 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
 // a half volume that is a multiple of kSiteBlock and fewer than 2^31 complex per vector
 bool hop16_pairs_supported(int nc, int m, int prec);
 bool hop16_blocked_supported(int nc, int m, int prec, int64_t vh);
+// one-time kernel attributes of the two-RHS kernel; call outside graph capture
+int hop16_pairs_prepare();
 
 // the kernel kind forced by qcuSetHopKernel (QCU_HOP_AUTO: none), and the automatic choice
 // (tuner record, else the static rule) for a shape

@@ -422,6 +422,12 @@ int launch16d_m(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     return QCU_SUCCESS;
 }
 
+// 8-byte asynchronous global -> shared copy (cp.async, completion by wait_group)
+__device__ __forceinline__ void cp_async8(uint2* smem, const uint2* gmem) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(a), "l"(gmem) : "memory");
+}
+
 // packed FP32 pair arithmetic (add.rn.f32x2 / sub: sm_100): one instruction per complex add
 __device__ __forceinline__ uint64_t f2_bits(float2 v) {
     return (uint64_t)__float_as_uint(v.x) | ((uint64_t)__float_as_uint(v.y) << 32);
@@ -558,7 +564,6 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
     const int j = threadIdx.x % M2;                // RHS pair
     const int64_t vh = p.g.vh;
     const int parity = p.parity;
-    constexpr int64_t site_len = (int64_t)kNs * NC * MR;   // words per site
     const uint2* __restrict__ in2 = reinterpret_cast<const uint2*>(p.in) + j;
     const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
     const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
@@ -579,14 +584,24 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
         if constexpr (BLK) return (n / kSiteBlock) * (kNs * NC * kSiteBlock * M2) + (n % kSiteBlock) * M2;
         else return n * (kNs * NC * M2);
     };
+    // Epilogue operands (x, and r0 where the epilogue reads it) are copied into shared memory
+    // with cp.async when a site starts, so the copies land while its 8 hops compute and hold
+    // no registers.  Layout [operand][row][thread] in 8-byte words; every thread reads back
+    // only the words it copied itself, so no block barrier is needed.
+    constexpr int NX = EPI == EPI_PLAIN ? 0 : ((EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 2 : 1);
+    extern __shared__ uint2 h16_epi[];
+    const int nthr = blockDim.x;
     for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / M2 + threadIdx.x / M2; site < vh; site += site_stride) {
-        if constexpr (EPI != EPI_PLAIN && !BLK) {
-            const int64_t off = (int64_t)j * 32;
-            if (off < site_len) {
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.x) + site * site_len + off));
-                if (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID)
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const uint32_t*>(p.r0) + site * site_len + off));
+        if constexpr (NX > 0) {
+            const int64_t b2 = sbase(site) + j;
+#pragma unroll
+            for (int r = 0; r < kNs * NC; ++r) {
+                cp_async8(&h16_epi[r * nthr + threadIdx.x], reinterpret_cast<const uint2*>(p.x) + b2 + r * RS);
+                if constexpr (NX == 2)
+                    cp_async8(&h16_epi[(kNs * NC + r) * nthr + threadIdx.x],
+                              reinterpret_cast<const uint2*>(p.r0) + b2 + r * RS);
             }
+            asm volatile("cp.async.commit_group;" ::: "memory");
         }
         const SiteXYZT c = site_coords(p.g, (uint32_t)site);
         const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
@@ -635,9 +650,8 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
         }
         // epilogue: the two RHS of every (spin, colour) row as one 8-byte word pair
         uint2* __restrict__ out2 = reinterpret_cast<uint2*>(p.out);
-        const uint2* __restrict__ x2 = reinterpret_cast<const uint2*>(p.x);
-        const uint2* __restrict__ r02 = reinterpret_cast<const uint2*>(p.r0);
         const int64_t base2 = sbase(site) + j;
+        if constexpr (NX > 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
         for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -647,9 +661,9 @@ __global__ void __launch_bounds__(kH16Threads, 2) hop16p_kernel(const HopParams 
                     const S2 a0 = St<S>::cv(acc[0][s][cc]), a1 = St<S>::cv(acc[1][s][cc]);
                     out2[o] = make_uint2(bits(a0), bits(a1));
                 } else {
-                    const uint2 xw = x2[o];
+                    const uint2 xw = h16_epi[(s * NC + cc) * nthr + threadIdx.x];
                     uint2 yw = make_uint2(0u, 0u);
-                    if (EPI == EPI_RESID || EPI == EPI_SCHUR_R0) yw = r02[o];
+                    if (EPI == EPI_RESID || EPI == EPI_SCHUR_R0) yw = h16_epi[(kNs * NC + s * NC + cc) * nthr + threadIdx.x];
                     uint32_t res_bits[2];
 #pragma unroll
                     for (int r = 0; r < 2; ++r) {
@@ -705,9 +719,11 @@ int launch16p_l(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
     }
     constexpr int M2 = MR / 2;
     const int block = (kH16Threads / M2) * M2;
-    int grid = resident_grid(k, block, p.g.vh * M2);
+    const int nx = epi == EPI_PLAIN ? 0 : ((epi == EPI_SCHUR_R0 || epi == EPI_RESID) ? 2 : 1);
+    const size_t smem = (size_t)nx * kNs * NC * block * sizeof(uint2);   // at most 48 KB
+    int grid = resident_grid(k, block, p.g.vh * M2, smem);
     if (grid > kScratchBlocks) grid = kScratchBlocks;
-    k<<<grid, block, 0, st>>>(p);
+    k<<<grid, block, smem, st>>>(p);
     QCUB_CHECK_LAUNCH();
     return QCU_SUCCESS;
 }
@@ -768,6 +784,41 @@ bool hop16_pairs_supported(int nc, int m, int prec) {
     return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc == 3 && (m == 8 || m == 12 || m == 16);
 }
 
+// The epilogues that stage two operands (x and r0) use 47 KB of dynamic shared memory,
+// which with the reduction's static arrays is above the 48 KB a kernel gets without
+// opting in.  The opt-in is a function attribute; it is set once per process, outside
+// any graph capture (context creation, or the first direct launch).
+template <typename S, int MR, bool BLK>
+static cudaError_t hop16p_optin() {
+    constexpr size_t need = (size_t)2 * kNs * 3 * kH16Threads * sizeof(uint2);
+    cudaError_t e = cudaFuncSetAttribute(hop16p_kernel<3, S, false, EPI_SCHUR_R0, MR, BLK>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(hop16p_kernel<3, S, false, EPI_RESID, MR, BLK>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+    return e;
+}
+
+int hop16_pairs_prepare() {
+    static bool done = false;
+    if (done) return QCU_SUCCESS;
+    cudaError_t e = cudaSuccess;
+    auto all = [&](auto tag) {
+        using S = decltype(tag);
+        if (e == cudaSuccess) e = hop16p_optin<S, 8, false>();
+        if (e == cudaSuccess) e = hop16p_optin<S, 12, false>();
+        if (e == cudaSuccess) e = hop16p_optin<S, 16, false>();
+        if (e == cudaSuccess) e = hop16p_optin<S, 8, true>();
+        if (e == cudaSuccess) e = hop16p_optin<S, 12, true>();
+        if (e == cudaSuccess) e = hop16p_optin<S, 16, true>();
+    };
+    all(__half{});
+    all(__nv_bfloat16{});
+    if (e != cudaSuccess) return set_error(QCU_ERR_CUDA, "hop kernel shared-memory opt-in: %s", cudaGetErrorString(e));
+    done = true;
+    return QCU_SUCCESS;
+}
+
 bool hop16_blocked_supported(int nc, int m, int prec, int64_t vh) {
     return hop16_pairs_supported(nc, m, prec) && vh % kSiteBlock == 0 && vh * 4 * nc * m < ((int64_t)1 << 31);
 }
@@ -775,6 +826,7 @@ bool hop16_blocked_supported(int nc, int m, int prec, int64_t vh) {
 int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
     if (!hop16_pairs_supported(nc, p.m, prec))
         return set_error(QCU_ERR_UNSUPPORTED, "two-RHS packed hop: n_color %d, m %d", nc, p.m);
+    if (int rc = hop16_pairs_prepare()) return rc;
     if (p.blocked && !hop16_blocked_supported(nc, p.m, prec, p.g.vh))
         return set_error(QCU_ERR_UNSUPPORTED, "site-blocked layout: half volume %lld", (long long)p.g.vh);
     if (p.g.vh >= (int64_t)1 << 31) return set_error(QCU_ERR_UNSUPPORTED, "half volume beyond 2^31");

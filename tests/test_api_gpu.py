@@ -170,6 +170,33 @@ def test_mixed_precision_with_packed_hop(oracle_lib, sloppy, kind):
     assert np.all(true_rel <= tol)
 
 
+@pytest.mark.parametrize("m", [8, 12])
+@pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
+def test_mixed_precision_two_rhs_kernel(oracle_lib, sloppy, m):
+    """The product configuration of the mixed solver: SU(3) with an RHS count the two-RHS
+    packed kernel takes, so every sloppy hop (plain, and the Schur forms that stage x and
+    r0 in shared memory and reduce) runs in it.  Same convergence as with the one-RHS
+    packed kernel (identical arithmetic per RHS) and the FP64 true residual."""
+    L, nc, kappa, tol = (8, 8, 8, 8), 3, 0.124, 1e-10
+    out = {}
+    for kind in (q.HOP_PACKED16_PAIRS, q.HOP_PACKED16):
+        q.check(q.lib().qcuSetHopKernel(kind))
+        try:
+            gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 16, kind="smooth", t_boundary=-1.0,
+                                             opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy,
+                                                   "reliable_delta": 0.003})
+        finally:
+            q.lib().qcuSetHopKernel(q.HOP_AUTO)
+        assert st == q.SUCCESS, _LAST["error"]
+        res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+        true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+        assert np.all(true_rel <= tol)
+        out[kind] = (x, stats.iterations)
+    (xp, itp), (xg, itg) = out[q.HOP_PACKED16_PAIRS], out[q.HOP_PACKED16]
+    assert abs(itp - itg) <= 2
+    assert rel_err(xp, xg) <= 1e-9
+
+
 @pytest.mark.parametrize("true_rule", [0, 1], ids=["schur_rule", "true_rule"])
 def test_cgnr_matches_oracle(oracle_lib, true_rule):
     """QCU_SOLVER_CGNR: CG on A^dag A x = A^dag b' follows the oracle's CGNR iterate by

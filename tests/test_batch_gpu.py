@@ -23,6 +23,7 @@ SYSTEMS = [
     ((6, 4, 4, 4), 2, 1, 0.11, 23),
     ((8, 8, 8, 8), 3, 4, 0.10, 24),
     ((4, 2, 2, 4), 4, 5, 0.115, 25),
+    ((8, 8, 4, 8), 3, 12, 0.12, 26),   # the two-RHS packed kernel in the mixed solves
 ]
 TOL = 1e-10
 
