@@ -42,9 +42,11 @@ WORKLOAD = "24^3x48 SU(3) Wilson-Dirac, N_rhs=12, kappa=0.124, smoothed links ep
 # Plain FP64 BiCGStab iterations this system needs (measured with this benchmark's
 # plain leg on a B200); the CPU reference leg multiplies its per-iteration time by it.
 PLAIN_ITERS = 44
-# reliable-update threshold of the mixed solves (a sweep over 0.1 .. 0.003 on this
-# system gave the shortest time at 0.003 for FP16, BF16 and FP32 sloppy storage)
-RELIABLE_DELTA = 0.003
+# reliable-update rule of the mixed solves per sloppy storage: threshold delta and the
+# fraction of the RHS that must meet it (a sweep of delta 0.1 .. 0.001 and quorum 0, 0.5,
+# 1 on this system: FP16 is fastest at 0.003 with every RHS waiting for the others, 4
+# reliable updates instead of 8; BF16 at 0.01, where the quorum changes little)
+RELIABLE = {"f16": (0.003, 1.0), "bf16": (0.01, 1.0)}
 CHECK_INTERVAL = 16
 # DRAM bytes of one hop launch on this workload (dram__bytes.sum.per_second x
 # gpu__time_duration from one ncu capture of the kernel at this size, plain epilogue);
@@ -241,12 +243,13 @@ def main():
         o.stop_true_residual = 1
         o.t_boundary = T_BOUNDARY
         o.check_interval = CHECK_INTERVAL
-        o.reliable_delta = RELIABLE_DELTA
+        key = "bf16" if sloppy == q.BF16 else "f16"
+        o.reliable_delta, o.reliable_quorum = RELIABLE[key]
         q.check(lib.qcuSetSolverOptions(ctypes.byref(o)))
 
     # hop kernel per (N, m, precision) picked by the autotuner before anything is timed
     tuned = {}
-    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs"}
+    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16"}
     for name, prec in (("f64", q.DOUBLE), ("f16", q.HALF), ("bf16", q.BF16)):
         if args.static_kernels:
             k = lib.qcuGetTunedHop(NC, M, prec)   # 0 (nothing recorded): the static rule applies
@@ -420,7 +423,7 @@ def main():
             "data": "synthetic: seeded smoothed SU(3) links exp(i 0.3 H), unit complex Gaussian sources",
             "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA,
                        "tol": TOL, "l2": "inputs larger than L2 (each hop reads 478 MB in BF16, 1.9 GB in FP64)",
-                       "replicas": world, "reliable_delta": RELIABLE_DELTA, "check_interval": CHECK_INTERVAL,
+                       "replicas": world, "reliable_delta_quorum": RELIABLE, "check_interval": CHECK_INTERVAL,
                        "hop_kernels": tuned},
             "solves_per_s_all_ranks": world / t_mixed,
             "mixed": {"iterations": it_mixed[-1], "reliable_updates": reliable, "true_residual_max": max(rel_mixed)},

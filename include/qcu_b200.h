@@ -67,6 +67,10 @@ typedef struct {
     int check_interval;      /* iterations per captured graph between host checks (8) */
     int freeze_converged;    /* 1: converged right-hand sides stop updating */
     int max_restarts;        /* MIXED: cap on reliable updates (0 = unlimited) */
+    double reliable_quorum;  /* MIXED: a reliable update waits until this fraction of the
+                                unconverged RHS met the delta rule or claim convergence
+                                (0: any one RHS, the default); an RHS whose sloppy residual
+                                fell below delta^2 * max ||r|| forces the update */
 } QcuSolverOptions;
 
 void qcuGetDefaultSolverOptions(QcuSolverOptions *opts);
@@ -282,6 +286,7 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
 #define QCU_HOP_PACKED16_ACC16 5
 #define QCU_HOP_PACKED16_STAGED 6
 #define QCU_HOP_PACKED16_PAIRS 7
+#define QCU_HOP_MMA16 8
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

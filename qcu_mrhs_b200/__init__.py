@@ -24,7 +24,7 @@ SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR
 
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND, SOLVER_CGNR = 0, 1, 2, 3, 4
 (HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16, HOP_PACKED16_STAGED,
- HOP_PACKED16_PAIRS) = range(8)
+ HOP_PACKED16_PAIRS, HOP_MMA16) = range(9)
 MAX_RHS = 64
 
 
@@ -46,6 +46,7 @@ class QcuSolverOptions(ctypes.Structure):
         ("check_interval", ctypes.c_int),
         ("freeze_converged", ctypes.c_int),
         ("max_restarts", ctypes.c_int),
+        ("reliable_quorum", ctypes.c_double),
     ]
 
 

@@ -68,6 +68,7 @@ static void default_options(QcuSolverOptions* o) {
     o->check_interval = 8;
     o->freeze_converged = 0;
     o->max_restarts = 0;
+    o->reliable_quorum = 0.0;
 }
 
 void context_destroy(Context* c) {
@@ -654,7 +655,7 @@ int qcuDslashMrhsSiteBlocked(void* out, const void* in, const void* gauge, const
 
 int qcuSetHopKernel(int kind) {
     clear_error();
-    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_PACKED16_PAIRS)
+    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_MMA16)
         return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
     set_hop_kind(kind);
     return QCU_SUCCESS;

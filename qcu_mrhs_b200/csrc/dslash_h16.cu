@@ -50,6 +50,18 @@ __device__ __forceinline__ uint32_t times_i(uint32_t u) { return __byte_perm(u, 
 __device__ __forceinline__ uint32_t times_mi(uint32_t u) { return __byte_perm(u, 0, 0x1032) ^ 0x80000000u; }  // -i v
 __device__ __forceinline__ uint32_t bcast_re(uint32_t u) { return __byte_perm(u, 0, 0x1010); }
 __device__ __forceinline__ uint32_t bcast_im(uint32_t u) { return __byte_perm(u, 0, 0x3232); }
+// the same broadcasts through the half-pair intrinsics, which the compiler can fold into
+// the operand selection of the packed FMA that consumes them (no separate instruction)
+template <typename T2> __device__ __forceinline__ T2 lo2(uint32_t u);
+template <typename T2> __device__ __forceinline__ T2 hi2(uint32_t u);
+template <> __device__ __forceinline__ __half2 lo2<__half2>(uint32_t u) { return __low2half2(word<__half2>(u)); }
+template <> __device__ __forceinline__ __half2 hi2<__half2>(uint32_t u) { return __high2half2(word<__half2>(u)); }
+template <> __device__ __forceinline__ __nv_bfloat162 lo2<__nv_bfloat162>(uint32_t u) {
+    return __low2bfloat162(word<__nv_bfloat162>(u));
+}
+template <> __device__ __forceinline__ __nv_bfloat162 hi2<__nv_bfloat162>(uint32_t u) {
+    return __high2bfloat162(word<__nv_bfloat162>(u));
+}
 
 constexpr int kH16Threads = 256;
 constexpr int kH16MaxSites = 32;   // sites staged per block pass
@@ -491,10 +503,10 @@ __device__ __forceinline__ void h16_hop2(float2 (&acc)[2][4][NC], const uint2* _
             const uint2 l = link(c, k);
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
-                w0[r] = P::fma(word<T2>(bcast_re(h0[r][k])), word<T2>(l.x), w0[r]);
-                w0[r] = P::fma(word<T2>(bcast_im(h0[r][k])), word<T2>(l.y), w0[r]);
-                w1[r] = P::fma(word<T2>(bcast_re(h1[r][k])), word<T2>(l.x), w1[r]);
-                w1[r] = P::fma(word<T2>(bcast_im(h1[r][k])), word<T2>(l.y), w1[r]);
+                w0[r] = P::fma(lo2<T2>(h0[r][k]), word<T2>(l.x), w0[r]);
+                w0[r] = P::fma(hi2<T2>(h0[r][k]), word<T2>(l.y), w0[r]);
+                w1[r] = P::fma(lo2<T2>(h1[r][k]), word<T2>(l.x), w1[r]);
+                w1[r] = P::fma(hi2<T2>(h1[r][k]), word<T2>(l.y), w1[r]);
             }
         }
         constexpr float sg = (float)SG;

@@ -41,6 +41,8 @@ struct BicgScalars {
     int x_fresh;                        // 1: the next STEP_XR writes the FP32 increment instead of
                                         //    adding to it (it was just folded into the FP64 x)
     double delta;                       // update when ||r_j|| < delta * maxr_j
+    double quorum;                      // fraction of the active RHS that must meet the delta
+                                        // rule (0: any one RHS)
     double len_per_rhs;                 // complex elements per RHS of the sloppy vectors
     double scale[kMaxRhs];              // sloppy vectors hold scale_j * (FP64 quantity)
     double ratio[kMaxRhs];              // scale_new / scale_old of the last update
@@ -112,7 +114,8 @@ __device__ inline void run_finisher(const RedArgs& ra, int m, const double2* sum
         return;
     }
     __shared__ int s_flags[2];
-    if (tid == 0) { s_flags[0] = 1; s_flags[1] = 0; }   // all converged, breakdown
+    __shared__ int s_cnt[2];   // mixed: RHS that met the reliable-update rule, active RHS
+    if (tid == 0) { s_flags[0] = 1; s_flags[1] = 0; s_cnt[0] = 0; s_cnt[1] = 0; }   // all converged, breakdown
     __syncthreads();
     if (tid < m) {
         const int j = tid;
@@ -146,8 +149,12 @@ __device__ inline void run_finisher(const RedArgs& ra, int m, const double2* sum
                         const double rn = sqrt(rn2);
                         if (rn > sc->maxr[j]) sc->maxr[j] = rn;
                         const double sj = sc->scale[j];
+                        atomicAdd(&s_cnt[1], 1);
                         if (rn < sc->delta * sc->maxr[j] || rn2 <= sc->tol2 * sc->bfull2[j] * sj * sj)
-                            s_flags[0] = 0;   // reused below as "update needed" (inverted)
+                            atomicAdd(&s_cnt[0], 1);
+                        // far past the threshold: update whatever the quorum
+                        if (rn < sc->delta * sc->delta * sc->maxr[j])
+                            s_flags[0] = 0;   // reused below as "update forced" (inverted)
                         b = cdiv(cmul(sc->alpha[j], rho_new), sc->omega[j]);
                         b = cdiv(b, sc->rho[j]);
                         if (!cfinite(b) || !(b.x * b.x + b.y * b.y <= sc->beta_max * sc->beta_max) ||
@@ -184,7 +191,14 @@ __device__ inline void run_finisher(const RedArgs& ra, int m, const double2* sum
     if (tid == 0) {
         if (ra.fin == FIN_BETA && sc->mixed) {
             sc->iter += 1;
-            if (!s_flags[0] || s_flags[1]) sc->gate = 1;   // breakdown also forces an update
+            // enough RHS met the rule (any one with quorum 0), one is far past it, or a
+            // breakdown: schedule a reliable update
+            int need = 1;
+            if (sc->quorum > 0.0) {
+                need = (int)ceil(sc->quorum * (double)s_cnt[1] - 1e-9);
+                if (need < 1) need = 1;
+            }
+            if (s_cnt[0] >= need || !s_flags[0] || s_flags[1]) sc->gate = 1;
             if (s_flags[1]) sc->restart = 1;
             if (sc->iter >= sc->max_iter) { sc->status = 3; sc->done = 1; }
         } else if (ra.fin == FIN_BETA) {

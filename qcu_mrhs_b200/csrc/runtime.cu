@@ -127,6 +127,8 @@ int hop_tc_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cu
 bool hop16_supported(int nc, int m, int prec);
 bool hop16_pairs_supported(int nc, int m, int prec);
 int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
+bool hop_mma16_supported(int nc, int m, int prec);
+int hop_mma16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, bool staged,
                  cudaStream_t st);
 
@@ -156,6 +158,8 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
     if (kind == QCU_HOP_TENSOR && hop_tc_supported(nc, p.m, prec) &&
         reinterpret_cast<uintptr_t>(p.in) % 16 == 0)
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
+    if (kind == QCU_HOP_MMA16 && hop_mma16_supported(nc, p.m, prec))
+        return hop_mma16_launch(p, nc, prec, dagger, epi, st);
     if (kind == QCU_HOP_PACKED16_PAIRS && hop16_pairs_supported(nc, p.m, prec))
         return hop16_pairs_launch(p, nc, prec, dagger, epi, st);
     if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16 || kind == QCU_HOP_PACKED16_STAGED ||

@@ -101,6 +101,7 @@ int prepare_scalars(Context& c, BicgScalars* dsc, int max_iter, double tol, int 
     h.mixed = mixed;
     h.x_fresh = mixed;   // the sloppy increment starts from zero
     h.delta = c.opts.reliable_delta > 0 ? c.opts.reliable_delta : 0.1;
+    h.quorum = c.opts.reliable_quorum > 0 ? (c.opts.reliable_quorum < 1 ? c.opts.reliable_quorum : 1.0) : 0.0;
     h.beta_max = mixed && c.opts.sloppy_precision == QCU_PRECISION_HALF ? kMaxHalfBeta : 1e300;
     h.len_per_rhs = (double)c.half_len();
     for (int j = 0; j < c.m; ++j) {

@@ -11,6 +11,7 @@ namespace qcub {
 
 bool hop_tc_supported(int nc, int m, int prec);
 bool hop16_supported(int nc, int m, int prec);
+bool hop_mma16_supported(int nc, int m, int prec);
 bool hop16_pairs_supported(int nc, int m, int prec);
 void set_hop_kind(int k);
 int hop_kind();
@@ -104,7 +105,8 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
     const int saved = hop_kind();
     // PACKED16_ACC16 is not a candidate: it trades accuracy for speed, so only an explicit
     // request selects it
-    int kinds[5] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS};
+    int kinds[6] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
+                    QCU_HOP_MMA16};
     int best = QCU_HOP_SIMT;
     float best_ms = 1e30f;
     for (int kind : kinds) {
@@ -112,6 +114,7 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         if (kind == QCU_HOP_TENSOR && !hop_tc_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16 && !hop16_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16_PAIRS && !hop16_pairs_supported(nc, m, prec)) continue;
+        if (kind == QCU_HOP_MMA16 && !hop_mma16_supported(nc, m, prec)) continue;
         set_hop_kind(kind);
         HopParams p{};
         p.in = in;

@@ -197,6 +197,52 @@ def test_mixed_precision_two_rhs_kernel(oracle_lib, sloppy, m):
     assert rel_err(xp, xg) <= 1e-9
 
 
+@pytest.mark.parametrize("m", [8, 12, 16])
+@pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
+def test_mixed_precision_mma16_kernel(oracle_lib, sloppy, m):
+    """The mixed solver with every sloppy hop (plain and the reducing Schur forms) in the
+    warp-MMA kernel reaches the FP64 true residual and the solution of the two-RHS packed
+    kernel (different rounding inside the hop, same converged solution)."""
+    L, nc, kappa, tol = (8, 8, 8, 8), 3, 0.124, 1e-10
+    out = {}
+    for kind in (q.HOP_MMA16, q.HOP_PACKED16_PAIRS):
+        q.check(q.lib().qcuSetHopKernel(kind))
+        try:
+            gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 18, kind="smooth", t_boundary=-1.0,
+                                             opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy,
+                                                   "reliable_delta": 0.003})
+        finally:
+            q.lib().qcuSetHopKernel(q.HOP_AUTO)
+        assert st == q.SUCCESS, _LAST["error"]
+        res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+        true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+        assert np.all(true_rel <= tol)
+        out[kind] = (x, stats.iterations)
+    (xm, itm), (xp, itp) = out[q.HOP_MMA16], out[q.HOP_PACKED16_PAIRS]
+    assert abs(itm - itp) <= 0.25 * itp + 2
+    assert rel_err(xm, xp) <= 1e-7
+
+
+@pytest.mark.parametrize("quorum", [0.5, 1.0])
+@pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
+def test_mixed_precision_reliable_quorum(oracle_lib, sloppy, quorum):
+    """reliable_quorum: the reliable update waits until that fraction of the unconverged
+    RHS met the delta rule.  The solve still stops only on the FP64 true residual, and it
+    needs about as many reliable updates as the any-RHS rule on the same system, or fewer."""
+    L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 8, 0.124, 1e-10
+    updates = {}
+    for qr in (0.0, quorum):
+        gauge, b, x, st, stats = _invert(L, nc, m, kappa, tol, 17, kind="smooth", t_boundary=-1.0,
+                                         opts={"solver": q.SOLVER_MIXED, "sloppy_precision": sloppy,
+                                               "reliable_delta": 0.003, "reliable_quorum": qr})
+        assert st == q.SUCCESS, _LAST["error"]
+        res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+        true_rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+        assert np.all(true_rel <= tol)
+        updates[qr] = stats.reliable_updates
+    assert 1 <= updates[quorum] <= updates[0.0] + 1
+
+
 @pytest.mark.parametrize("true_rule", [0, 1], ids=["schur_rule", "true_rule"])
 def test_cgnr_matches_oracle(oracle_lib, true_rule):
     """QCU_SOLVER_CGNR: CG on A^dag A x = A^dag b' follows the oracle's CGNR iterate by

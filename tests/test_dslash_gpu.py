@@ -98,8 +98,8 @@ def _acc16_factor(kind, prec):
 
 
 LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16,
-                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS]
-LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"]
+                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS, q.HOP_MMA16]
+LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs", "mma16"]
 
 
 @pytest.mark.parametrize("hop_kernel", LOWP_KERNELS, indirect=True, ids=LOWP_IDS)
@@ -152,6 +152,38 @@ def test_low_precision_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel)
     assert q.lib().qcuGetKernelError(1) == 0
 
 
+@pytest.mark.parametrize("hop_kernel", [q.HOP_MMA16], indirect=True, ids=["mma16"])
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16])
+@pytest.mark.parametrize("m", [8, 12, 16])
+@pytest.mark.parametrize("L", [(2, 2, 2, 2), (6, 2, 4, 2), (8, 4, 4, 8)])
+def test_mma16_hop_shapes_and_epilogues(oracle_lib, prec, m, L, hop_kernel):
+    """The warp-MMA hop (one warp per site, FP32 accumulation in the tensor cores) at the RHS
+    counts it covers: both parities with and without dagger against the oracle on the same
+    rounded inputs, odd half volumes, tiny lattices, the xpay and Schur epilogues."""
+    nc = 3
+    gauge, inp = _problem(L, nc, m, 80 + m)
+    gr, ir = _round(gauge, prec), _round(inp, prec)
+    tol = TOL[prec]
+    for parity in (0, 1):
+        for dagger in (False, True):
+            ref = oracle_lib.hop(ir, gr, L, parity, dagger, -1.0)
+            got = _hop_gpu(inp, gauge, L, parity, dagger, -1.0, prec)
+            assert rel_err(got, ref) <= tol
+    x = F.to_mrhs(F.gaussian_fermions(L, nc, m, 81, parities=1)[:, 0])
+    xr = _round(x, prec)
+    d_in, d_g, d_x = to_dev(inp, prec), to_dev(gauge, prec), to_dev(x, prec)
+    d_out, d_tmp = empty_dev(inp.shape, prec), empty_dev(inp.shape, prec)
+    q.check(q.lib().qcuDslashMrhsXpay(d_out.data_ptr(), d_in.data_ptr(), d_g.data_ptr(), d_x.data_ptr(), -0.37,
+                                      q.lattice(L), nc, m, 1, 0, 1.0, prec, None))
+    sync()
+    assert rel_err(from_dev(d_out), xr - 0.37 * oracle_lib.hop(ir, gr, L, 1, False, 1.0)) <= tol
+    q.check(q.lib().qcuSchurMrhs(d_out.data_ptr(), d_in.data_ptr(), d_tmp.data_ptr(), d_g.data_ptr(), 0.11,
+                                 q.lattice(L), nc, m, -1.0, prec, None))
+    sync()
+    assert rel_err(from_dev(d_out), oracle_lib.schur(ir, gr, L, 0.11, -1.0)) <= 2 * tol
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
 @pytest.mark.parametrize("hop_kernel", [q.HOP_SIMT, q.HOP_SIMT_CS], indirect=True, ids=["simt", "simt_cs"])
 @pytest.mark.parametrize("nc,m", [(3, 4), (3, 12), (6, 8), (8, 16), (8, 32), (5, 3)])
 def test_fp64_hop_kernels(oracle_lib, nc, m, hop_kernel):
@@ -174,10 +206,11 @@ def test_autotuner_records_a_valid_choice(tmp_path, monkeypatch):
     L = (8, 4, 4, 8)
     for prec in (q.DOUBLE, q.BF16):
         k = q.lib().qcuTuneHop(q.lattice(L), 3, 12, prec, None)
-        assert k in (q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16), q.last_error()
+        assert k in (q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_PAIRS,
+                     q.HOP_MMA16), q.last_error()
         assert q.lib().qcuGetTunedHop(3, 12, prec) == k
         if prec == q.DOUBLE:
-            assert k not in (q.HOP_TENSOR, q.HOP_PACKED16)
+            assert k not in (q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_PAIRS, q.HOP_MMA16)
     assert q.lib().qcuTuneHop(q.lattice((7, 4, 4, 4)), 3, 12, q.DOUBLE, None) < 0
 
 
