@@ -207,20 +207,26 @@ __global__ void __launch_bounds__(kMmaThreads, 2) hop_mma16_kernel(const HopPara
         for (int k = 0; k < (NV > 0 ? NV : 1); ++k) red[q][k] = make_float2(0.f, 0.f);
 
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; site < vh; site += nwarps) {
+    // neighbour half-site indices of a site (forward, backward per direction) and whether
+    // its t hops cross the boundary
+    auto neighbours = [&](int64_t site, uint32_t (&nb)[8], bool& wf_t, bool& wb_t) {
         const SiteXYZT c = site_coords(p.g, (uint32_t)site);
         const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
-        int64_t nbr[8];
-        nbr[0] = site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh);
-        nbr[1] = site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1));
-        nbr[2] = site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy);
-        nbr[3] = site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy);
-        nbr[4] = site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz);
-        nbr[5] = site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz);
-        const bool wf_t = (c.t + 1 == Lt), wb_t = (c.t == 0);
-        nbr[6] = site + (wf_t ? -(int64_t)(Lt - 1) * st : st);
-        nbr[7] = site + (wb_t ? (int64_t)(Lt - 1) * st : -st);
-
+        nb[0] = (uint32_t)(site - c.xh + (xodd ? (c.xh + 1 == lxh ? 0 : c.xh + 1) : c.xh));
+        nb[1] = (uint32_t)(site - c.xh + (xodd ? c.xh : (c.xh == 0 ? lxh - 1 : c.xh - 1)));
+        nb[2] = (uint32_t)(site + (c.y + 1 == Ly ? -(int64_t)(Ly - 1) * sy : sy));
+        nb[3] = (uint32_t)(site + (c.y == 0 ? (int64_t)(Ly - 1) * sy : -sy));
+        nb[4] = (uint32_t)(site + (c.z + 1 == Lz ? -(int64_t)(Lz - 1) * sz : sz));
+        nb[5] = (uint32_t)(site + (c.z == 0 ? (int64_t)(Lz - 1) * sz : -sz));
+        wf_t = (c.t + 1 == Lt);
+        wb_t = (c.t == 0);
+        nb[6] = (uint32_t)(site + (wf_t ? -(int64_t)(Lt - 1) * st : st));
+        nb[7] = (uint32_t)(site + (wb_t ? (int64_t)(Lt - 1) * st : -st));
+    };
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; site < vh; site += nwarps) {
+        uint32_t nbr[8];
+        bool wf_t, wb_t;
+        neighbours(site, nbr, wf_t, wb_t);
         float d[4][4];
 #pragma unroll
         for (int s = 0; s < 4; ++s)
@@ -228,8 +234,8 @@ __global__ void __launch_bounds__(kMmaThreads, 2) hop_mma16_kernel(const HopPara
             for (int k = 0; k < 4; ++k) d[s][k] = 0.f;
 
         auto load_dir = [&](int mu, uint2 (&qf)[4], uint2 (&qb)[4], uint32_t& wf, uint32_t& wb) {
-            const uint2* pf = reinterpret_cast<const uint2*>(in + nbr[2 * mu] * SITE + lofs);
-            const uint2* pb = reinterpret_cast<const uint2*>(in + nbr[2 * mu + 1] * SITE + lofs);
+            const uint2* pf = reinterpret_cast<const uint2*>(in + (int64_t)nbr[2 * mu] * SITE + lofs);
+            const uint2* pb = reinterpret_cast<const uint2*>(in + (int64_t)nbr[2 * mu + 1] * SITE + lofs);
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 qf[s] = ld_ok ? __ldg(pf + s * (NC * MR / 2)) : make_uint2(0u, 0u);
@@ -238,20 +244,18 @@ __global__ void __launch_bounds__(kMmaThreads, 2) hop_mma16_kernel(const HopPara
             const uint32_t ff = (mu == 3 && wf_t) ? tflip : 0u;
             const uint32_t fb = (mu == 3 && wb_t) ? tflip : 0u;
             wf = w_ok ? (__ldg(gf + mu * gmu + site * N2 + woff) ^ ff) : 0u;
-            wb = w_ok ? (__ldg(gb + mu * gmu + nbr[2 * mu + 1] * N2 + woff_b) ^ 0x80000000u ^ fb) : 0u;
+            wb = w_ok ? (__ldg(gb + mu * gmu + (int64_t)nbr[2 * mu + 1] * N2 + woff_b) ^ 0x80000000u ^ fb) : 0u;
         };
-        {
-            // all 8 neighbours' words and links are requested before the first MMA, so a
-            // site costs one memory round trip instead of four
-            uint2 qf[4][4], qb[4][4];
-            uint32_t wf[4], wb[4];
+        // all 8 neighbours' words and links are requested before the first MMA, so a site
+        // costs one memory round trip instead of four
+        uint2 qf[4][4], qb[4][4];
+        uint32_t wf[4], wb[4];
 #pragma unroll
-            for (int mu = 0; mu < 4; ++mu) load_dir(mu, qf[mu], qb[mu], wf[mu], wb[mu]);
-            mma_dir<S, 0, SF>(d, qf[0], qb[0], wf[0], wb[0], e);
-            mma_dir<S, 1, SF>(d, qf[1], qb[1], wf[1], wb[1], e);
-            mma_dir<S, 2, SF>(d, qf[2], qb[2], wf[2], wb[2], e);
-            mma_dir<S, 3, SF>(d, qf[3], qb[3], wf[3], wb[3], e);
-        }
+        for (int mu = 0; mu < 4; ++mu) load_dir(mu, qf[mu], qb[mu], wf[mu], wb[mu]);
+        mma_dir<S, 0, SF>(d, qf[0], qb[0], wf[0], wb[0], e);
+        mma_dir<S, 1, SF>(d, qf[1], qb[1], wf[1], wb[1], e);
+        mma_dir<S, 2, SF>(d, qf[2], qb[2], wf[2], wb[2], e);
+        mma_dir<S, 3, SF>(d, qf[3], qb[3], wf[3], wb[3], e);
         (void)SB;
 
         // epilogue: lane (g, t) owns colour t of RHS 2g (d[s][0..1]) and 2g+1 (d[s][2..3])
