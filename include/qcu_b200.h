@@ -277,7 +277,10 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *            shared by the pair), SU(3) with m = 8, 12 or 16 (else PACKED16);
  *   MMA16    FP16/BF16, SU(3), m = 8, 12 or 16: one warp per site, the forward and
  *            backward hop of a direction as one mma.sync m16n8k16 per output spin (link
- *            products in the tensor cores, FP32 accumulation); else as AUTO;
+ *            products in the tensor cores, FP32 accumulation); else as AUTO.  Only an
+ *            explicit request selects it: its Schur and residual forms, most of the
+ *            solver's hops, are slower than PACKED16_PAIRS's, which the autotuner's
+ *            plain-hop timing does not see;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else PACKED16_PAIRS, PACKED16 or SIMT,
  *            the first that applies. */

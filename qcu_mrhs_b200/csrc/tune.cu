@@ -11,7 +11,6 @@ namespace qcub {
 
 bool hop_tc_supported(int nc, int m, int prec);
 bool hop16_supported(int nc, int m, int prec);
-bool hop_mma16_supported(int nc, int m, int prec);
 bool hop16_pairs_supported(int nc, int m, int prec);
 void set_hop_kind(int k);
 int hop_kind();
@@ -104,9 +103,11 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
     fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(gauge), (int64_t)(gauge_bytes / 4), 2u);
     const int saved = hop_kind();
     // PACKED16_ACC16 is not a candidate: it trades accuracy for speed, so only an explicit
-    // request selects it
-    int kinds[6] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
-                    QCU_HOP_MMA16};
+    // request selects it.  Nor is MMA16: the tuner times the plain hop, where MMA16 can be
+    // the faster one, but its Schur and residual forms (two of the four hops of a solver
+    // iteration) are slower than PACKED16_PAIRS's, and the solve with it is slower (B200,
+    // 24^3x48, m = 12, FP16: 87.3 ms against 81.6 ms)
+    int kinds[5] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS};
     int best = QCU_HOP_SIMT;
     float best_ms = 1e30f;
     for (int kind : kinds) {
@@ -114,7 +115,6 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         if (kind == QCU_HOP_TENSOR && !hop_tc_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16 && !hop16_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16_PAIRS && !hop16_pairs_supported(nc, m, prec)) continue;
-        if (kind == QCU_HOP_MMA16 && !hop_mma16_supported(nc, m, prec)) continue;
         set_hop_kind(kind);
         HopParams p{};
         p.in = in;
