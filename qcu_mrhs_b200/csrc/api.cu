@@ -74,6 +74,7 @@ static void default_options(QcuSolverOptions* o) {
 void context_destroy(Context* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->iter_exec) cudaGraphExecDestroy(c->iter_exec);
     scratch_free(&c->ws);
     if (c->host_sc) cudaFreeHost(c->host_sc);
     if (c->ev0) cudaEventDestroy(c->ev0);

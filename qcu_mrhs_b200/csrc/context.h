@@ -54,6 +54,9 @@ struct Context {
     DevBuf scalars;           // BicgScalars (device)
     BicgScalars* host_sc = nullptr;   // pinned mirror
     Precond* precond = nullptr;       // learned preconditioner (not owned), QCU_SOLVER_PRECOND
+    // executable graph of the last Schur solve's iteration block, updated in place from
+    // each new capture (owned)
+    cudaGraphExec_t iter_exec = nullptr;
 
     int64_t half_len() const { return g.vh * 4 * nc; }               // complex per RHS per parity
     size_t half_bytes(int prec) const { return (size_t)half_len() * m * 2 * prec_bytes(prec); }

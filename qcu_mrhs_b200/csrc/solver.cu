@@ -72,6 +72,40 @@ int capture(Context& c, int count, const std::function<int()>& body, cudaGraphEx
     return QCU_SUCCESS;
 }
 
+// Capture `count` calls of body into *exec, reusing the executable graph *exec already
+// holds when the new capture has its topology (cudaGraphExecUpdate copies every node's
+// parameters from the new capture, so the result is the same as a fresh instantiation);
+// otherwise, or when the update is refused, instantiate anew.  Saves the instantiation of
+// the iteration block on every solve after the first of a context.
+int capture_cached(Context& c, int count, const std::function<int()>& body, cudaGraphExec_t* exec) {
+    if (!*exec) return capture(c, count, body, exec);
+    cudaGraph_t graph = nullptr;
+    QCUB_CUDA_CHECK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = QCU_SUCCESS;
+    for (int i = 0; i < count && rc == QCU_SUCCESS; ++i) rc = body();
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+    if (rc != QCU_SUCCESS) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return set_error(QCU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(*exec, graph, &info) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return QCU_SUCCESS;
+    }
+    cudaGetLastError();   // a refused update is not an error of this call
+    cudaGraphExecDestroy(*exec);
+    *exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        *exec = nullptr;
+        return set_error(QCU_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+    }
+    return QCU_SUCCESS;
+}
+
 // Run the captured iteration block until the device sets `done`.
 int run_graph(Context& c, cudaGraphExec_t exec, BicgScalars* dsc) {
     for (;;) {
@@ -362,11 +396,8 @@ int solve_one(Context& c, void* x, const void* b, int max_iter, double tol, bool
     int rc = solve.begin(x, b, max_iter, tol);
     if (rc) return rc;
     const int interval = c.opts.check_interval > 0 ? c.opts.check_interval : 8;
-    cudaGraphExec_t exec = nullptr;
-    if ((rc = capture(c, interval, [&]() { return solve.enqueue_iteration(); }, &exec))) return rc;
-    rc = run_graph(c, exec, solve.device_scalars());
-    cudaGraphExecDestroy(exec);
-    if (rc) return rc;
+    if ((rc = capture_cached(c, interval, [&]() { return solve.enqueue_iteration(); }, &c.iter_exec))) return rc;
+    if ((rc = run_graph(c, c.iter_exec, solve.device_scalars()))) return rc;
     return solve.end();
 }
 
