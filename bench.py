@@ -249,7 +249,7 @@ def main():
 
     # hop kernel per (N, m, precision) picked by the autotuner before anything is timed
     tuned = {}
-    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16"}
+    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16", 9: "mma_link"}
     for name, prec in (("f64", q.DOUBLE), ("f16", q.HALF), ("bf16", q.BF16)):
         if args.static_kernels:
             k = lib.qcuGetTunedHop(NC, M, prec)   # 0 (nothing recorded): the static rule applies
@@ -334,34 +334,31 @@ def main():
     gen = torch.Generator(device="cpu").manual_seed(11)
     psi64 = torch.randn((vh, 4, NC, M, 2), generator=gen, dtype=torch.float64).cuda()
     ref_out = torch.empty_like(psi64)
-    q.check(lib.qcuDslashMrhs(ref_out.data_ptr(), psi64.data_ptr(), d_gauge.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
-                              q.DOUBLE, dev_stream))
+    # the context's own hop (qcuDslashMrhsContext): the kernel, gauge copy and per-site tables
+    # the solver uses
+    q.check(lib.qcuDslashMrhsContext(ref_out.data_ptr(), psi64.data_ptr(), 0, 0, q.DOUBLE, dev_stream))
     dslash_err = {}
     for name, prec, dt in (("f16", q.HALF, torch.float16), ("bf16", q.BF16, torch.bfloat16),
                            ("f32", q.SINGLE, torch.float32), ("f64", q.DOUBLE, torch.float64)):
         s_b = q.PREC_BYTES[prec]
-        g_l = d_gauge.to(dt)
         a = psi64.to(dt)
         out = torch.empty_like(a)
-        q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
-                                  prec, dev_stream))
+        q.check(lib.qcuDslashMrhsContext(out.data_ptr(), a.data_ptr(), 0, 0, prec, dev_stream))
         torch.cuda.synchronize()
         if prec != q.DOUBLE:
             dslash_err[name] = float(torch.linalg.vector_norm(out.double() - ref_out) /
                                      torch.linalg.vector_norm(ref_out))
         if name == "f32":
-            del g_l, a, out
+            del a, out
             continue
         for _ in range(3):
-            q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, 0, 0, T_BOUNDARY,
-                                      prec, dev_stream))
+            q.check(lib.qcuDslashMrhsContext(out.data_ptr(), a.data_ptr(), 0, 0, prec, dev_stream))
         reps = 20
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
         for i in range(reps):
-            q.check(lib.qcuDslashMrhs(out.data_ptr(), a.data_ptr(), g_l.data_ptr(), Lc, NC, M, i & 1, 0,
-                                      T_BOUNDARY, prec, dev_stream))
+            q.check(lib.qcuDslashMrhsContext(out.data_ptr(), a.data_ptr(), i & 1, 0, prec, dev_stream))
         e1.record(stream)
         torch.cuda.synchronize()
         dur = e0.elapsed_time(e1) / 1e3 / reps
@@ -371,7 +368,7 @@ def main():
                       "launch_us": dur * 1e6,
                       "algorithmic_bytes": byts, "gflops": hop_flops(vh, NC, M) / dur / 1e9,
                       "kernel": tuned[name], "peak_kind": f"{peak_kind} HBM copy bandwidth"}
-        del g_l, a, out
+        del a, out
     del psi64, ref_out
 
     # ---- end to end through the C ABI with host buffers ----

@@ -181,6 +181,15 @@ int qcuDslashMrhsXpay(void *out, const void *in, const void *gauge, const void *
                       const int L[4], int n_color, int m_rhs, int parity, int dagger, double t_sign,
                       int precision, void *stream);
 
+/* qcuDslashMrhs on the gauge field of the qcu.h context (initGridSize, loadQcuGauge,
+ * getDslash), its lattice, n_color, m_rhs and t boundary (qcuSetSolverOptions), in
+ * `precision`: the hop the context's solver runs, including, for the FP16/BF16 tensor-core
+ * kernel, its per-site neighbour table and hop-link array (built on first use).  For
+ * callers that keep their own gathered multi-RHS fields.  Counterpart of calling the
+ * reference's qcu::Dslash::apply on the Qcu object's gauge copies
+ * (src/qcu_interface.cu:109-172 without the gather/scatter). */
+int qcuDslashMrhsContext(void *out, const void *in, int parity, int dagger, int precision, void *stream);
+
 /* Schur operator out_o = in_o - kappa^2 D_oe D_eo in_o; tmp is one half-lattice vector.
  * Replaces fused_x_sub_Doe_Deo_x -- reference src/solver/bicgstab_solve.cu:27-70. */
 int qcuSchurMrhs(void *out, const void *in, void *tmp, const void *gauge, double kappa,
@@ -281,6 +290,11 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *            explicit request selects it: its Schur and residual forms, most of the
  *            solver's hops, are slower than PACKED16_PAIRS's, which the autotuner's
  *            plain-hop timing does not see;
+ *   MMA_LINK FP16/BF16, 2 <= n_color <= 4, any m_rhs: one warp per (site, up to 16 RHS),
+ *            the links as the A operand of mma.sync m16n8k16 and the projected neighbour
+ *            half spinors (columns = RHS x half spinor) as B; the forward and backward hop
+ *            of a direction are one MMA per 4 RHS, link products and all sums in FP32, the
+ *            spin projection the only 16-bit arithmetic; else as AUTO;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else PACKED16_PAIRS, PACKED16 or SIMT,
  *            the first that applies. */
@@ -293,6 +307,7 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
 #define QCU_HOP_PACKED16_STAGED 6
 #define QCU_HOP_PACKED16_PAIRS 7
 #define QCU_HOP_MMA16 8
+#define QCU_HOP_MMA_LINK 9
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

@@ -24,7 +24,7 @@ SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR
 
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND, SOLVER_CGNR = 0, 1, 2, 3, 4
 (HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16, HOP_PACKED16_STAGED,
- HOP_PACKED16_PAIRS, HOP_MMA16) = range(9)
+ HOP_PACKED16_PAIRS, HOP_MMA16, HOP_MMA_LINK) = range(10)
 MAX_RHS = 64
 
 
@@ -114,6 +114,7 @@ _SIGNATURES = {
     "qcuBatchRelease": (_i, []),
     "qcuDslashMrhs": (_i, [_vp, _vp, _vp, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuDslashMrhsXpay": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _i, _i, _d, _i, _vp]),
+    "qcuDslashMrhsContext": (_i, [_vp, _vp, _i, _i, _i, _vp]),
     "qcuSchurMrhs": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _d, _i, _vp]),
     "qcuGatherMrhs": (_i, [_vp, _i, ctypes.POINTER(_vp), _i, _i64, _i, _i, _vp]),
     "qcuScatterMrhs": (_i, [ctypes.POINTER(_vp), _i, _vp, _i, _i64, _i, _i, _vp]),

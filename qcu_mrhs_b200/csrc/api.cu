@@ -56,6 +56,29 @@ int Context::gauge_in(int prec, const void** out) {
     return QCU_SUCCESS;
 }
 
+int Context::hop_tables(int prec, double t_sign, const void** links_out, const uint32_t** nbr_out) {
+    const void* gp = nullptr;
+    int rc = gauge_in(prec, &gp);
+    if (rc) return rc;
+    if (!nbr_valid) {
+        if ((rc = nbr.ensure(neighbour_table_bytes(g)))) return rc;
+        if ((rc = build_neighbour_table(static_cast<uint32_t*>(nbr.ptr), nbr.bytes, g, stream))) return rc;
+        nbr_valid = true;
+    }
+    if (!links_valid[prec] || links_tsign[prec] != t_sign) {
+        // both output parities: 2 x Vh x 8 links, twice the gauge field
+        if ((rc = links[prec].ensure(hop_links_bytes(g, nc, prec)))) return rc;
+        if ((rc = build_hop_links(links[prec].ptr, links[prec].bytes, gp, static_cast<const uint32_t*>(nbr.ptr), g, nc,
+                                  prec, t_sign, stream)))
+            return rc;
+        links_valid[prec] = true;
+        links_tsign[prec] = t_sign;
+    }
+    *links_out = links[prec].ptr;
+    *nbr_out = static_cast<const uint32_t*>(nbr.ptr);
+    return QCU_SUCCESS;
+}
+
 static std::mutex g_api;
 static Context* g_ctx = nullptr;
 
@@ -113,6 +136,7 @@ int context_init(Context* c, const int L[4], int n_color, int m_rhs, int in_prec
         rc = set_error(QCU_ERR_ALLOC, "pinned host allocation failed");
     }
     if (!rc) rc = hop16_pairs_prepare();   // before any solve is captured into a graph
+    if (!rc) rc = hop_mmal_prepare();
     return rc;
 }
 
@@ -123,7 +147,7 @@ int context_load_gauge(Context* c, const void* gauge, int prec) {
     int rc;
     if ((rc = c->gauge[D].ensure((size_t)c->gauge_len() * 16))) return rc;
     if ((rc = cast_complex(c->gauge[D].ptr, D, gauge, prec, c->gauge_len(), c->stream))) return rc;
-    for (int i = 0; i < 5; ++i) c->gauge_valid[i] = false;
+    for (int i = 0; i < 5; ++i) c->gauge_valid[i] = c->links_valid[i] = false;
     c->gauge_valid[D] = true;
     c->gauge_loaded = true;
     return QCU_SUCCESS;
@@ -227,7 +251,12 @@ static int start_dslash_impl(int parity, int dagger) {
         ins[j] = c.queue[j].second;
     }
     if ((rc = gather_mrhs(c.mrhs_in.ptr, Pd, ins, c.in_prec, c.g.vh, c.nc, c.m, c.stream))) return rc;
+    const void* links = nullptr;
+    const uint32_t* nbr = nullptr;
+    if (hop_reads_tables(c.nc, c.m, Pd) && (rc = c.hop_tables(Pd, c.opts.t_boundary, &links, &nbr))) return rc;
     HopParams p{};
+    p.links = links;
+    p.nbr = nbr;
     p.out = c.mrhs_out.ptr;
     p.in = c.mrhs_in.ptr;
     p.gauge = gauge;
@@ -265,8 +294,13 @@ static int mat_impl(int dagger) {
     char* gout = static_cast<char*>(c.mrhs_out.ptr);
     for (int par = 0; par < 2; ++par)
         if ((rc = gather_mrhs(gin + par * hb, Pd, ins[par], c.in_prec, c.g.vh, c.nc, c.m, c.stream))) return rc;
+    const void* links = nullptr;
+    const uint32_t* nbr = nullptr;
+    if (hop_reads_tables(c.nc, c.m, Pd) && (rc = c.hop_tables(Pd, c.opts.t_boundary, &links, &nbr))) return rc;
     for (int par = 0; par < 2; ++par) {
         HopParams p{};
+        p.links = links;
+        p.nbr = nbr;
         p.out = gout + par * hb;
         p.in = gin + (1 - par) * hb;
         p.x = gin + par * hb;
@@ -491,6 +525,38 @@ int qcuDslashMrhsXpay(void* out, const void* in, const void* gauge, const void* 
                       EPI_XPAY);
 }
 
+int qcuDslashMrhsContext(void* out, const void* in, int parity, int dagger, int precision, void* stream) {
+    QCUB_API_BEGIN
+    int rc = require_ctx();
+    if (rc) return rc;
+    Context& c = *g_ctx;
+    if ((rc = require_dslash(c))) return rc;
+    if (!out || !in) return set_error(QCU_ERR_INVALID, "null pointer");
+    if (parity != 0 && parity != 1) return set_error(QCU_ERR_INVALID, "parity %d", parity);
+    const void* gauge = nullptr;
+    if ((rc = c.gauge_in(precision, &gauge))) return rc;
+    const void* links = nullptr;
+    const uint32_t* nbr = nullptr;
+    if (hop_reads_tables(c.nc, c.m, precision) &&
+        (rc = c.hop_tables(precision, c.opts.t_boundary, &links, &nbr)))
+        return rc;
+    // the gauge copy and tables were made on the context's stream: order the caller's after it
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    QCUB_CUDA_CHECK(cudaEventRecord(c.ev_in, c.stream));
+    QCUB_CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_in, 0));
+    HopParams p{};
+    p.out = out;
+    p.in = in;
+    p.gauge = gauge;
+    p.links = links;
+    p.nbr = nbr;
+    p.g = c.g;
+    p.m = c.m;
+    p.parity = parity;
+    p.t_sign = c.opts.t_boundary;
+    return hop_launch(p, c.nc, precision, dagger != 0, EPI_PLAIN, st);
+}
+
 int qcuSchurMrhs(void* out, const void* in, void* tmp, const void* gauge, double kappa, const int L[4],
                  int n_color, int m_rhs, double t_sign, int precision, void* stream) {
     clear_error();
@@ -656,7 +722,7 @@ int qcuDslashMrhsSiteBlocked(void* out, const void* in, const void* gauge, const
 
 int qcuSetHopKernel(int kind) {
     clear_error();
-    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_MMA16)
+    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_MMA_LINK)
         return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
     set_hop_kind(kind);
     return QCU_SUCCESS;

@@ -36,6 +36,13 @@ struct Context {
     // gauge copies by precision code (index 0..4); the FP64 copy is the master
     DevBuf gauge[5];
     bool gauge_valid[5] = {false, false, false, false, false};
+    // per-site tables of the tensor-core hop (hop_tables.cu): neighbour table of the
+    // lattice, and hop-link arrays by precision with the t-boundary sign they were built for
+    DevBuf nbr;
+    bool nbr_valid = false;
+    DevBuf links[5];
+    bool links_valid[5] = {false, false, false, false, false};
+    double links_tsign[5] = {0, 0, 0, 0, 0};
 
     std::vector<std::pair<void*, void*>> queue;   // (out, in) pairs, reference order
 
@@ -64,6 +71,9 @@ struct Context {
 
     // gauge in `prec`, created from the FP64 master on first use
     int gauge_in(int prec, const void** out);
+    // neighbour table and hop-link array in `prec` for t-boundary sign t_sign, built on
+    // first use (outside graph capture)
+    int hop_tables(int prec, double t_sign, const void** links_out, const uint32_t** nbr_out);
 };
 
 // One Schur BiCGStab solve split into phases, so that several solves can share one
@@ -90,6 +100,8 @@ class SchurSolve {
     int P_ = 0, S_ = 0;                 // FP64/FP32 solve precision; sloppy precision
     const void* g_ = nullptr;           // gauge in P_
     const void* gs_ = nullptr;          // gauge in S_ (mixed)
+    const void* links_s_ = nullptr;     // per-site tables of the sloppy hop (or null)
+    const uint32_t* nbr_s_ = nullptr;
     char* x_ = nullptr;
     const char* b_ = nullptr;
     void* v_[11] = {};

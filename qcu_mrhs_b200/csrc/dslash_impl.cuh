@@ -47,6 +47,10 @@ struct HopParams {
     const int* done;   // if non-null and *done != 0 the kernel returns at once
     const int* gate;   // if non-null and *gate == 0 the kernel returns at once
     int blocked;       // 1: in, out, x and r0 in the site-blocked layout (kSiteBlock)
+    // optional per-site tables (hop_tables.cu), read by the tensor-core hop when both are set:
+    // hop-link array in the storage precision built for this t_sign, and neighbour table
+    const void* links;
+    const uint32_t* nbr;
 };
 
 __device__ __forceinline__ bool skip_launch(const int* done, const int* gate) {

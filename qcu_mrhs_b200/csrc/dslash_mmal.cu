@@ -1,0 +1,905 @@
+// dslash_mmal.cu -- multi-RHS hop term for FP16 / BF16 storage on the warp-level tensor-core
+// MMA (mma.sync m16n8k16, 16-bit operands, FP32 accumulation) with the LINKS as the A operand
+// and the projected neighbour spinors as the B operand.
+//
+// Same operator, layouts and epilogues as dslash_impl.cuh (reference
+// include/kernel/su_n_m_rhs_dslash.cuh:92-105, complex_matmul.cuh:16-600, whose solver hop
+// also runs the link products through tensor-core tiles).
+//
+// Work unit: one warp per (half-site, chunk of up to 16 RHS); inside it, groups of 4 RHS.
+// For direction mu, with the forward hop matrix W_f = U_mu(x) (t-boundary sign folded in)
+// and the backward one W_b = U_mu(x - mu)^dag, one real MMA per group of 4 RHS does both hops:
+//   K (16)   8 complex slots as (re, im) pairs: slot c = forward colour c, slot 4 + c =
+//            backward colour c (N <= 4; the rest zero)
+//   B (16x8) column j = (RHS j/2 of the group, half spinor j%2): the projected forward and
+//            backward neighbour half spinors h_f, h_b (lane 4g+t holds column g, colour t)
+//   A (16x16) rows 0..2N-1, "sum" rows (c', re/im):  [emb(W_f)      | emb(W_b)]
+//            rows 8..8+2N-1, "diff" rows (c', re/im): [emb(phi W_f) | emb(-phi W_b)]
+//   D        sum rows: W_f h_f + W_b h_b, which spins 0 and 1 take as they are (column
+//            h = 0 and 1); diff rows: phi (W_f h_f - W_b h_b), phi = the lower-spin phase of
+//            the forward projector (the backward projector's is -phi)
+// emb(W) is the real embedding [[W.re, -W.im], [W.im, W.re]] of each complex entry.  The
+// lower spins take the diff rows with a direction-dependent column (the x and y projectors
+// exchange the half spinors) and sign (y and z flip spin 3), so every direction has its
+// own D tile (4 FP32 per lane) and the tiles are added at the end, in FP32:
+//   spin0 = sum_mu D_mu[sum, h0]          spin1 = sum_mu D_mu[sum, h1]
+//   spin2 = D_x[diff,h1] + D_y[diff,h1] + D_z[diff,h0] + D_t[diff,h0]
+//   spin3 = D_x[diff,h0] - D_y[diff,h0] - D_z[diff,h1] + D_t[diff,h1]
+// So the link products and all sums are FP32; the only 16-bit arithmetic is the spin
+// projection (one rounding of p_a + kappa p_b, kappa in {+-1, +-i}) and the final store.
+//
+// Fragment layouts (PTX ISA, mma.m16n8k16, 16-bit A/B): lane = 4 g + t holds
+//   A: a0 = (row g, k 2t..2t+1), a1 = (row g+8, k 2t..), a2 = (row g, k 2t+8..), a3 = (row g+8, k 2t+8..)
+//   B: b0 = (k 2t..2t+1, col g), b1 = (k 2t+8..2t+9, col g)
+//   D: d0, d1 = (row g, col 2t..2t+1), d2, d3 = (row g+8, col 2t..2t+1)
+// so lane (g, t) builds its A words from the link elements W_f[g/2][t], W_b[g/2][t], loads
+// the neighbour words of (half spinor g%2, colour t, RHS g/2) and ends with component g%2
+// (re/im) of the four output spins of (colour g/2, RHS t).  Lanes g and g^1 (lane ^ 4)
+// exchange halves so that each stores two whole complex words.  Lanes outside the colour
+// range load clamped (finite) words that meet zero A entries, and store nothing.
+//
+// For 5 <= N <= 8 the sum and diff rows are two M tiles and the forward and backward
+// colours two K steps (4 MMAs per direction and group); the sum tile is shared by the
+// directions, the diff tiles are per direction.
+#include <type_traits>
+
+#include "dslash.h"
+#include "dslash_impl.cuh"
+#include "workspace.h"
+
+namespace qcub {
+
+int* device_error_flag();   // runtime.cu: per-device flag, nonzero after a timed-out wait
+
+namespace {
+
+constexpr int kLThreads = 256;
+constexpr int kLWarps = kLThreads / 32;
+constexpr int kLMaxChunkRhs = 16;   // RHS per work unit (4 groups of 4)
+
+template <typename S> struct LMma;
+template <> struct LMma<__half> {
+    static constexpr uint32_t kOne = 0x3C00u;
+    __device__ static void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
+                               float c1, float c2, float c3) {
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%10,%11,%12,%13};"
+            : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
+    }
+    __device__ static uint32_t fma(uint32_t a, uint32_t b, uint32_t c) {
+        const __half2 r = __hfma2(*reinterpret_cast<const __half2*>(&a), *reinterpret_cast<const __half2*>(&b),
+                                  *reinterpret_cast<const __half2*>(&c));
+        return *reinterpret_cast<const uint32_t*>(&r);
+    }
+    __device__ static uint32_t pack(float lo, float hi) {
+        const __half2 r = __floats2half2_rn(lo, hi);
+        return *reinterpret_cast<const uint32_t*>(&r);
+    }
+    __device__ static float2 unpack(uint32_t u) { return __half22float2(*reinterpret_cast<const __half2*>(&u)); }
+};
+template <> struct LMma<__nv_bfloat16> {
+    static constexpr uint32_t kOne = 0x3F80u;
+    __device__ static void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
+                               float c1, float c2, float c3) {
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%10,%11,%12,%13};"
+            : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
+    }
+    __device__ static uint32_t fma(uint32_t a, uint32_t b, uint32_t c) {
+        const __nv_bfloat162 r = __hfma2(*reinterpret_cast<const __nv_bfloat162*>(&a),
+                                         *reinterpret_cast<const __nv_bfloat162*>(&b),
+                                         *reinterpret_cast<const __nv_bfloat162*>(&c));
+        return *reinterpret_cast<const uint32_t*>(&r);
+    }
+    __device__ static uint32_t pack(float lo, float hi) {
+        const __nv_bfloat162 r = __floats2bfloat162_rn(lo, hi);
+        return *reinterpret_cast<const uint32_t*>(&r);
+    }
+    __device__ static float2 unpack(uint32_t u) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u));
+    }
+};
+
+// packed pair of +-1 in the 16-bit format (lo in the low half)
+template <typename S>
+__host__ __device__ constexpr uint32_t unit_pair(int lo, int hi) {
+    return (LMma<S>::kOne | (lo < 0 ? 0x8000u : 0u)) | ((LMma<S>::kOne | (hi < 0 ? 0x8000u : 0u)) << 16);
+}
+__device__ __forceinline__ uint32_t swap_halves(uint32_t u) { return __byte_perm(u, 0, 0x1032); }
+
+// phase codes: 0 = +1, 1 = -1, 2 = +i, 3 = -i
+__host__ __device__ constexpr int lphase(int s, bool imag) { return (imag ? 2 : 0) + (s > 0 ? 0 : 1); }
+// lower-spin phase of spin 2 for direction MU and projector sign SG (spin2 += C2 (W h)_{P2});
+// spin 3 takes +-C2 (W h)_{P3} (the tables of dslash_impl.cuh)
+template <int MU, int SG>
+struct LRecon {
+    static constexpr int C2 = MU == 0 ? lphase(-SG, true) : MU == 1 ? lphase(SG, false)
+                            : MU == 2 ? lphase(-SG, true) : lphase(SG, false);
+};
+// emb(c W) from e = emb(W) of this lane's row (re rows: (W.re, -W.im), im rows: (W.im, W.re)):
+//   emb(-W) = e ^ sign bits; emb(iW) = swap(e) ^ high sign; emb(-iW) = swap(e) ^ low sign
+template <int C>
+__device__ __forceinline__ uint32_t emb_phase(uint32_t e) {
+    if (C == 0) return e;
+    if (C == 1) return e ^ 0x80008000u;
+    if (C == 2) return swap_halves(e) ^ 0x80000000u;
+    return swap_halves(e) ^ 0x00008000u;
+}
+
+// Projection of one neighbour word pair for lane column h = g % 2 (see the kernel comment):
+//   MU 0: h = p_h + s i p_{3-h}      MU 1: h = p_h + (h ? s : -s) p_{3-h}
+//   MU 2: h = p_h + (h ? -s : s) i p_{2+h}      MU 3: h = p_h + s p_{2+h}
+// as one packed FMA p + mult * q (q swapped for the i cases); `lm` is the lane's multiplier
+// for MU 1 / MU 2 (it depends on h).
+template <typename S, int MU, int SG>
+__device__ __forceinline__ uint32_t lproject(uint32_t pw, uint32_t qw, uint32_t lm) {
+    using M = LMma<S>;
+    if (MU == 0) return M::fma(swap_halves(qw), unit_pair<S>(-SG, SG), pw);
+    if (MU == 1) return M::fma(qw, lm, pw);
+    if (MU == 2) return M::fma(swap_halves(qw), lm, pw);
+    return M::fma(qw, unit_pair<S>(SG, SG), pw);
+}
+
+// One direction for all groups of the work unit: the four neighbour words of every group
+// are requested first, then each group's two projections and one MMA that adds the forward
+// and backward hop into the direction class's FP32 accumulator quad through the MMA's C
+// operand (Q[n] is the x/y quad or the z/t quad of group n).
+template <typename S, int MU, int SF, int NTC, bool EXACT>
+__device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __restrict__ pf,
+                                         const uint32_t* __restrict__ qf, const uint32_t* __restrict__ pb,
+                                         const uint32_t* __restrict__ qb, const uint32_t (&A)[4], uint32_t lmf,
+                                         uint32_t lmb, int rb0, int q, int m) {
+    using M = LMma<S>;
+    constexpr int SB = -SF;
+    uint32_t w[NTC][4];
+#pragma unroll
+    for (int n = 0; n < NTC; ++n) {
+        if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
+        int d = 4 * n;
+        if (!EXACT) d += min(0, m - 1 - (rb0 + 4 * n + q));   // last partial group: clamp the RHS
+        w[n][0] = __ldg(pf + d);
+        w[n][1] = __ldg(qf + d);
+        w[n][2] = __ldg(pb + d);
+        w[n][3] = __ldg(qb + d);
+    }
+#pragma unroll
+    for (int n = 0; n < NTC; ++n) {
+        if (!EXACT && rb0 + 4 * n >= m) break;
+        const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
+        const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
+        M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
+    }
+}
+
+// A fragment of direction MU.  Rows are ordered (re/im, sum/diff, colour): lane (g, t) holds
+// rows g (re) and g + 8 (im) of class cls = g / 4 (0 sum, 1 diff) and colour g % 4, for
+// K slots t (forward colour t) and t + 4 (backward colour t).  wf = W_f[g%4][t] (t-boundary
+// sign folded in), wb = W_b[g%4][t] = conj(U_b[t][g%4]); diff lanes take phi W_f and -phi W_b,
+// applied as a lane byte permute (psel: identity or half swap) and sign mask (pmf / pmb).
+// emb re row: (w.re, -w.im) = w ^ high sign; im row: (w.im, w.re) = swap(w).
+__device__ __forceinline__ void mmal_a(uint32_t (&A)[4], uint32_t wf, uint32_t wb, uint32_t okm, uint32_t psel,
+                                       uint32_t pmf, uint32_t pmb) {
+    const uint32_t ff = (__byte_perm(wf, 0, psel) ^ pmf) & okm;
+    const uint32_t fb = (__byte_perm(wb, 0, psel) ^ pmb) & okm;
+    A[0] = ff ^ 0x80000000u;
+    A[1] = swap_halves(ff);
+    A[2] = fb ^ 0x80000000u;
+    A[3] = swap_halves(fb);
+}
+
+// lane phase constants of the diff rows for a direction whose forward lower-spin phase has
+// code C (0 = +1, 1 = -1, 2 = +i, 3 = -i): phi w = perm(w, sel) ^ mask (i w = swap(w) ^ low sign)
+struct LPhase {
+    uint32_t sel, mf, mb;
+};
+template <int C>
+__device__ __forceinline__ LPhase lphase_lane(bool diff) {
+    LPhase r;
+    constexpr bool imag = C >= 2;
+    constexpr uint32_t mpos = imag ? 0x00008000u : 0u;              // +1 or +i
+    constexpr uint32_t mneg = imag ? 0x80000000u : 0x80008000u;     // -1 or -i
+    constexpr bool neg = (C & 1) != 0;
+    r.sel = (diff && imag) ? 0x1032u : 0x3210u;
+    r.mf = diff ? (neg ? mneg : mpos) : 0u;
+    r.mb = diff ? (neg ? mpos : mneg) : 0u;   // backward: -phi
+    return r;
+}
+
+// Resident blocks per SM asked of the register allocator: 3 (80 registers) for the forms
+// without a reduction, 2 for the reducing forms (their epilogue words and partial sums
+// would spill at 80).
+template <int EPI> struct LMinBlocks {
+    static constexpr int value = (EPI == EPI_SCHUR_R0 || EPI == EPI_SCHUR_TS || EPI == EPI_RESID) ? 2 : 3;
+};
+
+template <typename S, int NC, bool DAG, int EPI, int NTC, bool EXACT, bool PRE>
+__global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_kernel(const HopParams p, int nchunk) {
+    using M = LMma<S>;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int NVR = NV > 0 ? NV : 1;
+    constexpr int NY = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : 0;   // reads r0 / y
+    constexpr uint32_t N2 = NC * NC;
+    constexpr int SF = DAG ? 1 : -1;   // forward projector 1 - s g: sign of gamma
+    static_assert(NC >= 2 && NC <= 4, "one M tile holds the sum and diff rows for N <= 4");
+    if (skip_launch(p.done, p.gate)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3, hh = g & 1, q = g >> 1;
+    const int cls = g >> 2, cc = g & 3;          // D/A rows of this lane: class, colour
+    const int m = p.m;
+    const uint32_t SW = 4u * NC * (uint32_t)m;   // 32-bit words per site
+    const int ccl = min(cc, NC - 1), ct = min(t, NC - 1);
+    const uint32_t okm = (cc < NC && t < NC) ? 0xffffffffu : 0u;   // this lane's A entries exist
+    const bool sok = cc < NC;                    // this lane's output colour exists
+    // input shifted to the lane's B column RHS (q of a group); the lane pointers to the words
+    // p_h, q of the projections follow once the chunk is known
+    const uint32_t* __restrict__ in = static_cast<const uint32_t*>(p.in) + q;
+    // output words of this lane: spins 2 cls, 2 cls + 1 of colour g % 4, RHS t of a group
+    const uint32_t os = (uint32_t)((2 * cls * NC + ccl) * m + t);
+    const uint32_t osn = (uint32_t)(NC * m);
+    // lane projection multipliers of MU 1 and MU 2 (forward / backward)
+    const uint32_t m1f = hh ? unit_pair<S>(SF, SF) : unit_pair<S>(-SF, -SF);
+    const uint32_t m2f = hh ? unit_pair<S>(SF, -SF) : unit_pair<S>(-SF, SF);
+    const uint32_t m1b = m1f ^ 0x80008000u, m2b = m2f ^ 0x80008000u;
+    // diff-row phases per direction, and the lane sign that flips spin 3 between the two
+    // directions of a class (diff lanes only)
+    const LPhase ph0 = lphase_lane<LRecon<0, SF>::C2>(cls != 0);
+    const LPhase ph1 = lphase_lane<LRecon<1, SF>::C2>(cls != 0);
+    const LPhase ph2 = lphase_lane<LRecon<2, SF>::C2>(cls != 0);
+    const LPhase ph3 = lphase_lane<LRecon<3, SF>::C2>(cls != 0);
+    const float fl = cls ? -1.f : 1.f;
+
+    const uint32_t vh = (uint32_t)p.g.vh;
+    const int parity = p.parity;
+    const uint32_t* __restrict__ gauge = static_cast<const uint32_t*>(p.gauge);
+    uint32_t* __restrict__ out = static_cast<uint32_t*>(p.out);
+    const uint32_t* __restrict__ xv = static_cast<const uint32_t*>(p.x);
+    const uint32_t* __restrict__ yv = static_cast<const uint32_t*>(p.r0);
+    const uint32_t gblk = vh * N2;   // words of one (mu, parity) block of the gauge
+    const uint32_t* __restrict__ glf = gauge + (size_t)parity * gblk + (uint32_t)(ccl * NC + ct);
+    const uint32_t* __restrict__ glb = gauge + (size_t)(1 - parity) * gblk + (uint32_t)(ct * NC + ccl);
+    const size_t gmu = 2 * (size_t)gblk;
+    const uint32_t tflip = p.t_sign < 0 ? 0x80008000u : 0u;
+    const uint32_t lxh = (uint32_t)p.g.lxh, Ly = (uint32_t)p.g.L[1], Lz = (uint32_t)p.g.L[2],
+                   Lt = (uint32_t)p.g.L[3];
+    const uint32_t sy = lxh, sz = lxh * Ly, st = sz * Lz;
+
+    // work units: warp gw takes chunk gw % nchunk of the sites gw / nchunk + k stride
+    const int64_t gw = (int64_t)blockIdx.x * kLWarps + warp;
+    const int64_t nw = (int64_t)gridDim.x * kLWarps;
+    const int chunk = (int)(gw % nchunk);
+    const uint32_t site_stride = (uint32_t)(nw / nchunk);
+    const uint32_t site0 = gw < (int64_t)site_stride * nchunk ? (uint32_t)(gw / nchunk) : vh;
+    const int rb0 = chunk * NTC * 4;
+    const uint32_t* __restrict__ inA = in + rb0 + (hh * NC + ct) * m;
+    const uint32_t* __restrict__ inB01 = in + rb0 + ((3 - hh) * NC + ct) * m;
+    const uint32_t* __restrict__ inB23 = in + rb0 + ((2 + hh) * NC + ct) * m;
+
+    float2 red[NTC][NVR];
+#pragma unroll
+    for (int n = 0; n < NTC; ++n)
+#pragma unroll
+        for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
+
+    for (uint32_t site = site0; site < vh; site += site_stride) {
+        // neighbours and the lane's link words W_f[g%4][t], W_b[g%4][t] of the 4 directions
+        uint32_t nb0, nb1, nb2, nb3, nb4, nb5, nb6, nb7;
+        uint32_t wf[4], wb[4];
+        if constexpr (PRE) {
+            const uint4* nt = reinterpret_cast<const uint4*>(p.nbr) + ((size_t)parity * vh + site) * 2;
+            const uint4 na = __ldg(nt), nc4 = __ldg(nt + 1);
+            nb0 = na.x; nb1 = na.y; nb2 = na.z; nb3 = na.w;
+            nb4 = nc4.x; nb5 = nc4.y; nb6 = nc4.z; nb7 = nc4.w;
+            const uint32_t* lk = static_cast<const uint32_t*>(p.links) + ((size_t)parity * vh + site) * 8 * N2 +
+                                 (uint32_t)(ccl * NC + ct);
+#pragma unroll
+            for (int mu = 0; mu < 4; ++mu) {
+                wf[mu] = __ldg(lk + 2 * mu * N2);
+                wb[mu] = __ldg(lk + (2 * mu + 1) * N2);
+            }
+        } else {
+            const SiteXYZT c = site_coords(p.g, site);
+            const uint32_t xh = (uint32_t)c.xh;
+            const int xodd = (parity ^ (c.y + c.z + c.t)) & 1;
+            const uint32_t row = site - xh;
+            nb0 = row + (xodd ? (xh + 1 == lxh ? 0u : xh + 1) : xh);
+            nb1 = row + (xodd ? xh : (xh == 0 ? lxh - 1 : xh - 1));
+            nb2 = site + sy - ((uint32_t)c.y + 1 == Ly ? Ly * sy : 0u);
+            nb3 = site - sy + ((uint32_t)c.y == 0 ? Ly * sy : 0u);
+            nb4 = site + sz - ((uint32_t)c.z + 1 == Lz ? Lz * sz : 0u);
+            nb5 = site - sz + ((uint32_t)c.z == 0 ? Lz * sz : 0u);
+            const bool wf_t = ((uint32_t)c.t + 1 == Lt), wb_t = (c.t == 0);
+            nb6 = site + st - (wf_t ? Lt * st : 0u);
+            nb7 = site - st + (wb_t ? Lt * st : 0u);
+            const uint32_t nbb[4] = {nb1, nb3, nb5, nb7};
+#pragma unroll
+            for (int mu = 0; mu < 4; ++mu) {
+                wf[mu] = __ldg(glf + mu * gmu + (size_t)site * N2);
+                wb[mu] = __ldg(glb + mu * gmu + (size_t)nbb[mu] * N2) ^ 0x80000000u;   // conj
+            }
+            if (wf_t) wf[3] ^= tflip;   // t-boundary sign
+            if (wb_t) wb[3] ^= tflip;
+        }
+        const size_t sbase = (size_t)site * SW + rb0;
+
+        // epilogue operands of this site, requested first
+        uint32_t xw[NTC][2], yw[NTC][2];
+        if constexpr (EPI != EPI_PLAIN) {
+#pragma unroll
+            for (int n = 0; n < NTC; ++n) {
+                xw[n][0] = xw[n][1] = yw[n][0] = yw[n][1] = 0u;
+                if (!EXACT && rb0 + 4 * n >= m) break;
+                if (sok && (EXACT || rb0 + 4 * n + t < m)) {
+                    const size_t o = sbase + os + 4 * n;
+                    xw[n][0] = __ldg(xv + o);
+                    xw[n][1] = __ldg(xv + o + osn);
+                    if (NY) {
+                        yw[n][0] = __ldg(yv + o);
+                        yw[n][1] = __ldg(yv + o + osn);
+                    }
+                }
+            }
+        }
+
+        float Qxy[NTC][4], Qzt[NTC][4];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Qxy[n][k] = Qzt[n][k] = 0.f;
+        uint32_t A[4];
+        // y, then spin 3 (diff column h0, registers 0 and 2) negated, then x: spin 3 takes
+        // x - y (the y projector's spin-3 phase is minus its diff-row phase)
+        mmal_a(A, wf[1], wb[1], okm, ph1.sel, ph1.mf, ph1.mb);
+        mmal_dir<S, 1, SF, NTC, EXACT>(Qxy, inA + (size_t)nb2 * SW, inB01 + (size_t)nb2 * SW, inA + (size_t)nb3 * SW,
+                                       inB01 + (size_t)nb3 * SW, A, m1f, m1b, rb0, q, m);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qxy[n][0] *= fl;
+            Qxy[n][2] *= fl;
+        }
+        mmal_a(A, wf[0], wb[0], okm, ph0.sel, ph0.mf, ph0.mb);
+        mmal_dir<S, 0, SF, NTC, EXACT>(Qxy, inA + (size_t)nb0 * SW, inB01 + (size_t)nb0 * SW, inA + (size_t)nb1 * SW,
+                                       inB01 + (size_t)nb1 * SW, A, 0u, 0u, rb0, q, m);
+        // z, then spin 3 (diff column h1, registers 1 and 3) negated, then t (boundary sign
+        // folded into the links)
+        mmal_a(A, wf[2], wb[2], okm, ph2.sel, ph2.mf, ph2.mb);
+        mmal_dir<S, 2, SF, NTC, EXACT>(Qzt, inA + (size_t)nb4 * SW, inB23 + (size_t)nb4 * SW, inA + (size_t)nb5 * SW,
+                                       inB23 + (size_t)nb5 * SW, A, m2f, m2b, rb0, q, m);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qzt[n][1] *= fl;
+            Qzt[n][3] *= fl;
+        }
+        mmal_a(A, wf[3], wb[3], okm, ph3.sel, ph3.mf, ph3.mb);
+        mmal_dir<S, 3, SF, NTC, EXACT>(Qzt, inA + (size_t)nb6 * SW, inB23 + (size_t)nb6 * SW, inA + (size_t)nb7 * SW,
+                                       inB23 + (size_t)nb7 * SW, A, 0u, 0u, rb0, q, m);
+
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
+            const bool rok = sok && (EXACT || rb0 + 4 * n + t < m);
+            const size_t o = sbase + os + 4 * n;
+            // the lane's two spins (2 cls, 2 cls + 1) of (colour g % 4, RHS t): sum lanes take
+            // both quads as they are; diff lanes take the x/y quad's columns crosswise (the
+            // x and y projectors exchange the half spinors)
+            float2 ov[2];
+            ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
+            ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
+            ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
+            ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
+            if (!rok) continue;
+            if constexpr (EPI == EPI_PLAIN) {
+                out[o] = M::pack(ov[0].x, ov[0].y);
+                out[o + osn] = M::pack(ov[1].x, ov[1].y);
+            } else {
+                const float a = (float)p.a;
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const float2 xx = M::unpack(xw[n][k]);
+                    float2 res;
+                    if (EPI == EPI_XPAY) {
+                        res = make_float2(xx.x + a * ov[k].x, xx.y + a * ov[k].y);
+                    } else if (EPI == EPI_RESID) {
+                        const float2 yy = M::unpack(yw[n][k]);
+                        res = make_float2(yy.x - xx.x + a * ov[k].x, yy.y - xx.y + a * ov[k].y);
+                    } else {
+                        res = make_float2(xx.x - a * ov[k].x, xx.y - a * ov[k].y);
+                    }
+                    const uint32_t rs = M::pack(res.x, res.y);
+                    out[o + (k ? osn : 0u)] = rs;
+                    if constexpr (NV > 0) {
+                        const float2 rr = M::unpack(rs);
+                        if (EPI == EPI_RESID) {
+                            red[n][0].x += rr.x * rr.x + rr.y * rr.y;
+                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
+                            const float2 qq = M::unpack(yw[n][k]);
+                            red[n][0].x += qq.x * rr.x + qq.y * rr.y;
+                            red[n][0].y += qq.x * rr.y - qq.y * rr.x;
+                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
+                            red[n][0].x += rr.x * xx.x + rr.y * xx.y;
+                            red[n][0].y += rr.x * xx.y - rr.y * xx.x;
+                            red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (NV > 0) {
+        // lanes (g, t) hold RHS rb0 + 4n + t: sum over g (fixed butterfly), then over the
+        // block's warps of the same chunk in order, then the common grid stage
+        __shared__ double2 wsum[kLWarps][NV][kLMaxChunkRhs];
+        __shared__ double2 bsum[NV * kMaxRhs];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                double vx = (double)red[n][k].x, vy = (double)red[n][k].y;
+#pragma unroll
+                for (int off = 4; off < 32; off <<= 1) {
+                    vx += __shfl_xor_sync(0xffffffffu, vx, off);
+                    vy += __shfl_xor_sync(0xffffffffu, vy, off);
+                }
+                if (g == 0) wsum[warp][k][4 * n + t] = make_double2(vx, vy);
+            }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NV * m; idx += blockDim.x) {
+            const int k = idx / m, rhs = idx - k * m;
+            const int ch = rhs / (4 * NTC), loc = rhs - ch * 4 * NTC;
+            double2 s = make_double2(0.0, 0.0);
+            for (int w = 0; w < kLWarps; ++w) {
+                if ((int)(((int64_t)blockIdx.x * kLWarps + w) % nchunk) != ch) continue;
+                s.x += wsum[w][k][loc].x;
+                s.y += wsum[w][k][loc].y;
+            }
+            bsum[idx] = s;
+        }
+        __syncthreads();
+        publish_and_finish<NV>(bsum, m, p.red);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Staged variant (the solver's hops: per-site tables present, m = 4, 8, 12 or 16).
+// Each warp keeps two shared-memory stages.  A stage holds the 8 neighbour site blocks
+// (16 N m bytes each, contiguous in the gathered layout), the site's hop-link block
+// (8 N^2 words) and, for the epilogues that read them, the site's x and r0 blocks.  While
+// the warp computes one site from one stage, the bulk-copy engine (cp.async.bulk, no
+// multicast) fills the other stage for the warp's next site: lanes 0-7 each copy one
+// neighbour block, lane 8 the links, lanes 9 and 10 x and r0; completion is counted in
+// bytes on the stage's mbarrier.  Fragment words are then read from shared memory at
+// compile-time offsets.  Every mbarrier wait is bounded: a wait that gives up sets the
+// device error flag, the warp drains its copies still in flight (again bounded) and skips
+// its remaining sites, so a broken pipeline ends the kernel with an error, never a hang.
+constexpr int kTWarps = 4;
+constexpr int kTThreads = kTWarps * 32;
+constexpr int kTStages = 2;
+constexpr int kTBarBytes = 64;   // mbarriers of the block (kTWarps x kTStages x 8 bytes)
+
+__device__ __forceinline__ uint32_t lsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool lbar_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > (1ll << 31)) return false;   // about a second
+    }
+}
+
+// Bytes of one stage: 8 neighbour blocks, the link block, NX epilogue blocks.
+__host__ __device__ constexpr int tstage_bytes(int nc, int m, int nx) { return (8 + nx) * 16 * nc * m + 32 * nc * nc; }
+
+template <typename S, int MU, int SF, int NTC>
+__device__ __forceinline__ void mmal_dir_s(float (&Q)[NTC][4], const uint32_t* pf, const uint32_t* qf,
+                                           const uint32_t* pb, const uint32_t* qb, const uint32_t (&A)[4],
+                                           uint32_t lmf, uint32_t lmb) {
+    using M = LMma<S>;
+    constexpr int SB = -SF;
+    uint32_t w[NTC][4];
+#pragma unroll
+    for (int n = 0; n < NTC; ++n) {
+        w[n][0] = pf[4 * n];
+        w[n][1] = qf[4 * n];
+        w[n][2] = pb[4 * n];
+        w[n][3] = qb[4 * n];
+    }
+#pragma unroll
+    for (int n = 0; n < NTC; ++n) {
+        const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
+        const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
+        M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
+    }
+}
+
+template <typename S, int NC, bool DAG, int EPI, int NTC>
+__global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams p, int* err) {
+    using M = LMma<S>;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int NVR = NV > 0 ? NV : 1;
+    constexpr int NX = EPI == EPI_PLAIN ? 0 : ((EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 2 : 1);
+    constexpr int MR = 4 * NTC;                  // RHS count
+    constexpr uint32_t N2 = NC * NC;
+    constexpr int SW = 4 * NC * MR;              // words of a site block
+    constexpr int SBY = 4 * SW;                  // its bytes
+    constexpr int LW = 8 * NC * NC;              // words of a link block
+    constexpr int STW = tstage_bytes(NC, MR, NX) / 4;
+    constexpr uint32_t TX = (uint32_t)tstage_bytes(NC, MR, NX);
+    constexpr int SF = DAG ? 1 : -1;
+    static_assert(NC >= 2 && NC <= 4 && MR <= 16, "staged hop: N <= 4, m <= 16");
+    extern __shared__ __align__(16) unsigned char tsm[];
+    if (skip_launch(p.done, p.gate)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3, hh = g & 1, q = g >> 1;
+    const int cls = g >> 2, cc = g & 3;
+    const int ccl = min(cc, NC - 1), ct = min(t, NC - 1);
+    const uint32_t okm = (cc < NC && t < NC) ? 0xffffffffu : 0u;
+    const bool sok = cc < NC;
+    const int oa = (hh * NC + ct) * MR + q;
+    const int ob01 = ((3 - hh) * NC + ct) * MR + q;
+    const int ob23 = ((2 + hh) * NC + ct) * MR + q;
+    const int os = (2 * cls * NC + ccl) * MR + t;
+    constexpr int osn = NC * MR;
+    const int lo = ccl * NC + ct;                // the lane's element of a link matrix
+    const uint32_t m1f = hh ? unit_pair<S>(SF, SF) : unit_pair<S>(-SF, -SF);
+    const uint32_t m2f = hh ? unit_pair<S>(SF, -SF) : unit_pair<S>(-SF, SF);
+    const uint32_t m1b = m1f ^ 0x80008000u, m2b = m2f ^ 0x80008000u;
+    const LPhase ph0 = lphase_lane<LRecon<0, SF>::C2>(cls != 0);
+    const LPhase ph1 = lphase_lane<LRecon<1, SF>::C2>(cls != 0);
+    const LPhase ph2 = lphase_lane<LRecon<2, SF>::C2>(cls != 0);
+    const LPhase ph3 = lphase_lane<LRecon<3, SF>::C2>(cls != 0);
+    const float fl = cls ? -1.f : 1.f;
+
+    const uint32_t vh = (uint32_t)p.g.vh;
+    const int parity = p.parity;
+    const unsigned char* __restrict__ in = static_cast<const unsigned char*>(p.in);
+    const unsigned char* __restrict__ links = static_cast<const unsigned char*>(p.links);
+    const unsigned char* __restrict__ xv = static_cast<const unsigned char*>(p.x);
+    const unsigned char* __restrict__ yv = static_cast<const unsigned char*>(p.r0);
+    const uint32_t* __restrict__ nbr = p.nbr + (size_t)parity * vh * 8;
+    uint32_t* __restrict__ out = static_cast<uint32_t*>(p.out);
+
+    // this warp's stages and barriers
+    uint32_t* stage = reinterpret_cast<uint32_t*>(tsm + kTBarBytes) + (size_t)warp * kTStages * STW;
+    const uint32_t bar0 = lsmem(tsm) + 8 * (warp * kTStages);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < kTStages; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * k) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+
+    const uint32_t gw = blockIdx.x * kTWarps + warp;
+    const uint32_t nw = gridDim.x * kTWarps;
+    // copy the blocks of `site` into stage k (lane 0 arms the barrier with the byte count;
+    // lanes 0-7 take neighbour nbi, lane 8 the links, lanes 9-10 the epilogue blocks)
+    auto issue = [&](int k, uint32_t site, uint32_t nbi) {
+        const uint32_t bar = bar0 + 8 * k;
+        if (lane == 0) asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TX) : "memory");
+        __syncwarp();
+        const unsigned char* src = nullptr;
+        uint32_t dst = lsmem(stage + k * STW), bytes = SBY;
+        if (lane < 8) {
+            src = in + (size_t)nbi * SBY;
+            dst += lane * SBY;
+        } else if (lane == 8) {
+            src = links + ((size_t)parity * vh + site) * (LW * 4);
+            dst += 8 * SBY;
+            bytes = LW * 4;
+        } else if (lane < 9 + NX) {
+            src = (lane == 9 ? xv : yv) + (size_t)site * SBY;
+            dst += 8 * SBY + LW * 4 + (lane - 9) * SBY;
+        }
+        if (src) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+        }
+    };
+
+    float2 red[NTC][NVR];
+#pragma unroll
+    for (int n = 0; n < NTC; ++n)
+#pragma unroll
+        for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
+
+    uint32_t site = gw;
+    uint32_t inflight = 0;   // bit k: stage k has copies in flight
+    uint32_t use = 0;        // uses of each stage so far (bit k = parity of stage k's next wait)
+    if (site < vh) {
+        issue(0, site, lane < 8 ? __ldg(nbr + (size_t)site * 8 + lane) : 0u);
+        inflight |= 1u;
+    }
+    // neighbour index of the next site, loaded one site ahead
+    uint32_t nb_next = (site + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(site + nw) * 8 + lane) : 0u;
+    bool ok = true;
+    for (int it = 0; site < vh; ++it, site += nw) {
+        const int k = it & 1;
+        const uint32_t nxt = site + nw;
+        if (nxt < vh) {   // the other stage was released by the previous site's __syncwarp
+            issue(k ^ 1, nxt, nb_next);
+            inflight |= 2u >> k;
+            nb_next = (nxt + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(nxt + nw) * 8 + lane) : 0u;
+        }
+        if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) {
+            ok = false;
+            break;
+        }
+        use ^= 1u << k;
+        inflight &= ~(1u << k);
+        const uint32_t* sb = stage + k * STW;       // neighbour blocks
+        const uint32_t* lk = sb + 8 * SW + lo;      // links
+        const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
+        float Qxy[NTC][4], Qzt[NTC][4];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
+        uint32_t A[4];
+        mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
+        mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
+                                  m1f, m1b);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qxy[n][0] *= fl;
+            Qxy[n][2] *= fl;
+        }
+        mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
+        mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u);
+        mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
+        mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
+                                  m2f, m2b);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qzt[n][1] *= fl;
+            Qzt[n][3] *= fl;
+        }
+        mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
+        mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
+                                  0u, 0u);
+        const size_t ob = (size_t)site * SW + os;
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            float2 ov[2];
+            ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
+            ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
+            ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
+            ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
+            if (!sok) continue;
+            if constexpr (EPI == EPI_PLAIN) {
+                out[ob + 4 * n] = M::pack(ov[0].x, ov[0].y);
+                out[ob + 4 * n + osn] = M::pack(ov[1].x, ov[1].y);
+            } else {
+                const float a = (float)p.a;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const uint32_t xw = ep[4 * n + (e ? osn : 0)];
+                    const float2 xx = M::unpack(xw);
+                    float2 res;
+                    if (EPI == EPI_XPAY) {
+                        res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
+                    } else if (EPI == EPI_RESID) {
+                        const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                        res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
+                    } else {
+                        res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
+                    }
+                    const uint32_t rs = M::pack(res.x, res.y);
+                    out[ob + 4 * n + (e ? osn : 0)] = rs;
+                    if constexpr (NV > 0) {
+                        const float2 rr = M::unpack(rs);
+                        if (EPI == EPI_RESID) {
+                            red[n][0].x += rr.x * rr.x + rr.y * rr.y;
+                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
+                            const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                            red[n][0].x += qq.x * rr.x + qq.y * rr.y;
+                            red[n][0].y += qq.x * rr.y - qq.y * rr.x;
+                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
+                            red[n][0].x += rr.x * xx.x + rr.y * xx.y;
+                            red[n][0].y += rr.x * xx.y - rr.y * xx.x;
+                            red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();   // every lane has read stage k before it is refilled
+    }
+    if (!ok) {
+        // a wait gave up: record it and let the copies still in flight land (bounded)
+        if (lane == 0) atomicExch(err, 1);
+        for (int k = 0; k < kTStages; ++k)
+            if ((inflight >> k) & 1u) {
+                if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) break;
+            }
+    }
+    if constexpr (NV > 0) {
+        __shared__ double2 wsum[kTWarps][NV][kLMaxChunkRhs];
+        __shared__ double2 bsum[NV * kMaxRhs];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                double vx = (double)red[n][k].x, vy = (double)red[n][k].y;
+#pragma unroll
+                for (int off = 4; off < 32; off <<= 1) {
+                    vx += __shfl_xor_sync(0xffffffffu, vx, off);
+                    vy += __shfl_xor_sync(0xffffffffu, vy, off);
+                }
+                if (g == 0) wsum[warp][k][4 * n + t] = make_double2(vx, vy);
+            }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NV * MR; idx += blockDim.x) {
+            const int k = idx / MR, rhs = idx - k * MR;
+            double2 s = make_double2(0.0, 0.0);
+            for (int w = 0; w < kTWarps; ++w) {
+                s.x += wsum[w][k][rhs].x;
+                s.y += wsum[w][k][rhs].y;
+            }
+            bsum[idx] = s;
+        }
+        __syncthreads();
+        publish_and_finish<NV>(bsum, MR, p.red);
+    }
+}
+
+template <typename S, int NC, int NTC, int EPI, bool DAG>
+void* tma_kernel_ptr() {
+    return reinterpret_cast<void*>(hop_mmal_tma_kernel<S, NC, DAG, EPI, NTC>);
+}
+
+template <typename S, int NC, int NTC>
+int launch_mmal_tma(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    void (*k)(const HopParams, int*) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop_mmal_tma_kernel<S, NC, true, EPI_PLAIN, NTC> : hop_mmal_tma_kernel<S, NC, false, EPI_PLAIN, NTC>; break;
+        case EPI_XPAY: k = dagger ? hop_mmal_tma_kernel<S, NC, true, EPI_XPAY, NTC> : hop_mmal_tma_kernel<S, NC, false, EPI_XPAY, NTC>; break;
+        case EPI_SCHUR_R0: k = hop_mmal_tma_kernel<S, NC, false, EPI_SCHUR_R0, NTC>; break;
+        case EPI_SCHUR_TS: k = hop_mmal_tma_kernel<S, NC, false, EPI_SCHUR_TS, NTC>; break;
+        case EPI_SCHUR: k = hop_mmal_tma_kernel<S, NC, false, EPI_SCHUR, NTC>; break;
+        case EPI_RESID: k = hop_mmal_tma_kernel<S, NC, false, EPI_RESID, NTC>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    const int nx = epi == EPI_PLAIN ? 0 : ((epi == EPI_SCHUR_R0 || epi == EPI_RESID) ? 2 : 1);
+    const size_t smem = kTBarBytes + (size_t)kTWarps * kTStages * tstage_bytes(NC, 4 * NTC, nx);
+    int* err = device_error_flag();
+    if (!err) return set_error(QCU_ERR_CUDA, "device error flag unavailable");
+    int grid = resident_grid(k, kTThreads, p.g.vh * 32, smem);
+    if (grid > kScratchBlocks) grid = kScratchBlocks;
+    k<<<grid, kTThreads, smem, st>>>(p, err);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
+template <typename S, int NC, int NTC, bool EXACT, bool PRE>
+int launch_mmal_t(const HopParams& p, bool dagger, int epi, int nchunk, cudaStream_t st) {
+    void (*k)(const HopParams, int) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop_mmal_kernel<S, NC, true, EPI_PLAIN, NTC, EXACT, PRE> : hop_mmal_kernel<S, NC, false, EPI_PLAIN, NTC, EXACT, PRE>; break;
+        case EPI_XPAY: k = dagger ? hop_mmal_kernel<S, NC, true, EPI_XPAY, NTC, EXACT, PRE> : hop_mmal_kernel<S, NC, false, EPI_XPAY, NTC, EXACT, PRE>; break;
+        case EPI_SCHUR_R0: k = hop_mmal_kernel<S, NC, false, EPI_SCHUR_R0, NTC, EXACT, PRE>; break;
+        case EPI_SCHUR_TS: k = hop_mmal_kernel<S, NC, false, EPI_SCHUR_TS, NTC, EXACT, PRE>; break;
+        case EPI_SCHUR: k = hop_mmal_kernel<S, NC, false, EPI_SCHUR, NTC, EXACT, PRE>; break;
+        case EPI_RESID: k = hop_mmal_kernel<S, NC, false, EPI_RESID, NTC, EXACT, PRE>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    int grid = resident_grid(k, kLThreads, p.g.vh * nchunk * 32);
+    if (grid > kScratchBlocks) grid = kScratchBlocks;
+    k<<<grid, kLThreads, 0, st>>>(p, nchunk);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
+// the staged kernel's blocks are 16-byte aligned in global memory
+inline bool lalign16(const void* ptr) { return reinterpret_cast<uintptr_t>(ptr) % 16 == 0; }
+
+template <typename S, int NC, int NTC>
+int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, cudaStream_t st) {
+    const bool pre = p.links != nullptr && p.nbr != nullptr;
+    if (pre && nchunk == 1 && p.m == 4 * NTC && lalign16(p.in) && lalign16(p.links) &&
+        (!p.x || lalign16(p.x)) && (!p.r0 || lalign16(p.r0)))
+        return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
+    if (p.m == 4 * NTC * nchunk)
+        return pre ? launch_mmal_t<S, NC, NTC, true, true>(p, dagger, epi, nchunk, st)
+                   : launch_mmal_t<S, NC, NTC, true, false>(p, dagger, epi, nchunk, st);
+    return pre ? launch_mmal_t<S, NC, NTC, false, true>(p, dagger, epi, nchunk, st)
+               : launch_mmal_t<S, NC, NTC, false, false>(p, dagger, epi, nchunk, st);
+}
+
+template <typename S, int NC>
+int launch_mmal_nc(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    // groups of 4 RHS, at most 4 groups per work unit; chunks balanced
+    const int groups = (p.m + 3) / 4;
+    const int nchunk = (groups + 3) / 4;
+    const int ntc = (groups + nchunk - 1) / nchunk;
+    switch (ntc) {
+        case 1: return launch_mmal_f<S, NC, 1>(p, dagger, epi, nchunk, st);
+        case 2: return launch_mmal_f<S, NC, 2>(p, dagger, epi, nchunk, st);
+        case 3: return launch_mmal_f<S, NC, 3>(p, dagger, epi, nchunk, st);
+        default: return launch_mmal_f<S, NC, 4>(p, dagger, epi, nchunk, st);
+    }
+}
+
+template <typename S>
+int launch_mmal(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st) {
+    switch (nc) {
+        case 2: return launch_mmal_nc<S, 2>(p, dagger, epi, st);
+        case 3: return launch_mmal_nc<S, 3>(p, dagger, epi, st);
+        default: return launch_mmal_nc<S, 4>(p, dagger, epi, st);
+    }
+}
+
+}  // namespace
+
+namespace {
+template <typename S, int NC, int NTC>
+cudaError_t mmal_tma_optin() {
+    const int need = kTBarBytes + kTWarps * kTStages * tstage_bytes(NC, 4 * NTC, 2);
+    const void* ks[8] = {tma_kernel_ptr<S, NC, NTC, EPI_PLAIN, false>(), tma_kernel_ptr<S, NC, NTC, EPI_PLAIN, true>(),
+                         tma_kernel_ptr<S, NC, NTC, EPI_XPAY, false>(), tma_kernel_ptr<S, NC, NTC, EPI_XPAY, true>(),
+                         tma_kernel_ptr<S, NC, NTC, EPI_SCHUR_R0, false>(),
+                         tma_kernel_ptr<S, NC, NTC, EPI_SCHUR_TS, false>(),
+                         tma_kernel_ptr<S, NC, NTC, EPI_SCHUR, false>(), tma_kernel_ptr<S, NC, NTC, EPI_RESID, false>()};
+    for (const void* k : ks) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+template <typename S, int NC>
+cudaError_t mmal_tma_optin_nc() {
+    cudaError_t e = mmal_tma_optin<S, NC, 1>();
+    if (e == cudaSuccess) e = mmal_tma_optin<S, NC, 2>();
+    if (e == cudaSuccess) e = mmal_tma_optin<S, NC, 3>();
+    if (e == cudaSuccess) e = mmal_tma_optin<S, NC, 4>();
+    return e;
+}
+}  // namespace
+
+// One-time set-up of the staged kernel (shared-memory opt-in above 48 KB, the device error
+// flag); call outside graph capture.
+int hop_mmal_prepare() {
+    static bool done = false;
+    if (done) return QCU_SUCCESS;
+    cudaError_t e = mmal_tma_optin_nc<__half, 2>();
+    if (e == cudaSuccess) e = mmal_tma_optin_nc<__half, 3>();
+    if (e == cudaSuccess) e = mmal_tma_optin_nc<__half, 4>();
+    if (e == cudaSuccess) e = mmal_tma_optin_nc<__nv_bfloat16, 2>();
+    if (e == cudaSuccess) e = mmal_tma_optin_nc<__nv_bfloat16, 3>();
+    if (e == cudaSuccess) e = mmal_tma_optin_nc<__nv_bfloat16, 4>();
+    if (e != cudaSuccess) return set_error(QCU_ERR_CUDA, "staged hop shared-memory opt-in: %s", cudaGetErrorString(e));
+    if (!device_error_flag()) return set_error(QCU_ERR_CUDA, "device error flag unavailable");
+    done = true;
+    return QCU_SUCCESS;
+}
+
+bool hop_mmal_supported(int nc, int m, int prec) {
+    return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc >= 2 && nc <= 4 && m >= 1 &&
+           m <= kMaxRhs;
+}
+
+int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
+    if (!hop_mmal_supported(nc, p.m, prec))
+        return set_error(QCU_ERR_UNSUPPORTED, "link-operand tensor-core hop: n_color=%d m_rhs=%d precision=%d", nc,
+                         p.m, prec);
+    if (dagger && epi != EPI_PLAIN && epi != EPI_XPAY)
+        return set_error(QCU_ERR_UNSUPPORTED, "dagger hop only with plain/xpay epilogue");
+    if ((epi != EPI_PLAIN && !p.x) || ((epi == EPI_SCHUR_R0 || epi == EPI_RESID) && !p.r0))
+        return set_error(QCU_ERR_INVALID, "link-operand tensor-core hop: epilogue operand missing");
+    // 32-bit word offsets: every spinor word index below 2^31
+    if (p.g.vh * 4 * nc * (int64_t)p.m >= ((int64_t)1 << 31) || p.g.vh * 8 * nc * nc >= ((int64_t)1 << 31))
+        return set_error(QCU_ERR_UNSUPPORTED, "link-operand tensor-core hop: field beyond 2^31 complex");
+    if (prec == QCU_PRECISION_HALF) return launch_mmal<__half>(p, nc, dagger, epi, st);
+    return launch_mmal<__nv_bfloat16>(p, nc, dagger, epi, st);
+}
+
+}  // namespace qcub

@@ -129,6 +129,8 @@ bool hop16_pairs_supported(int nc, int m, int prec);
 int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 bool hop_mma16_supported(int nc, int m, int prec);
 int hop_mma16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
+bool hop_mmal_supported(int nc, int m, int prec);
+int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, bool staged,
                  cudaStream_t st);
 
@@ -147,6 +149,13 @@ static int hop_nc(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t
     }
 }
 
+bool hop_reads_tables(int nc, int m, int prec) {
+    if (prec != QCU_PRECISION_HALF && prec != QCU_PRECISION_BF16) return false;
+    int kind = g_hop_kind;
+    if (kind == QCU_HOP_AUTO) kind = auto_hop_kind(nc, m, prec);
+    return kind == QCU_HOP_MMA_LINK && hop_mmal_supported(nc, m, prec);
+}
+
 int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
     if (p.m < 1 || p.m > kMaxRhs) return set_error(QCU_ERR_INVALID, "m_rhs=%d outside [1, %d]", p.m, kMaxRhs);
     if (p.g.L[0] % 2 || p.g.L[0] < 2 || p.g.L[1] < 1 || p.g.L[2] < 1 || p.g.L[3] < 1)
@@ -160,6 +169,8 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
     if (kind == QCU_HOP_MMA16 && hop_mma16_supported(nc, p.m, prec))
         return hop_mma16_launch(p, nc, prec, dagger, epi, st);
+    if (kind == QCU_HOP_MMA_LINK && hop_mmal_supported(nc, p.m, prec))
+        return hop_mmal_launch(p, nc, prec, dagger, epi, st);
     if (kind == QCU_HOP_PACKED16_PAIRS && hop16_pairs_supported(nc, p.m, prec))
         return hop16_pairs_launch(p, nc, prec, dagger, epi, st);
     if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16 || kind == QCU_HOP_PACKED16_STAGED ||

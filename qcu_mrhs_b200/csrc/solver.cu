@@ -34,6 +34,14 @@ struct Hop {
     Context& c;
     int prec;
     const void* gauge;
+    const void* links = nullptr;   // per-site tables of the tensor-core hop (or null)
+    const uint32_t* nbr = nullptr;
+    // fetch (build on first use) the per-site tables when the hop kernel for this shape
+    // reads them; call outside graph capture
+    int tables() {
+        if (!hop_reads_tables(c.nc, c.m, prec)) return QCU_SUCCESS;
+        return c.hop_tables(prec, c.opts.t_boundary, &links, &nbr);
+    }
     int launch(void* out, const void* in, int parity, int epi, const void* x = nullptr,
                const void* r0 = nullptr, double a = 0.0, int fin = FIN_NONE, BicgScalars* sc = nullptr,
                double2* result = nullptr, const int* done = nullptr, const int* gate = nullptr) {
@@ -51,6 +59,8 @@ struct Hop {
         p.red = RedArgs{c.ws.partials, c.ws.counter, result ? result : c.ws.result, sc, nullptr, fin};
         p.done = done;
         p.gate = gate;
+        p.links = links;
+        p.nbr = nbr;
         return hop_launch(p, c.nc, prec, false, epi, c.stream);
     }
 };
@@ -278,6 +288,12 @@ int SchurSolve::begin_mixed(int max_iter, double tol) {
     int rc;
     if ((rc = c.gauge_in(P_, &g_))) return rc;
     if ((rc = c.gauge_in(S_, &gs_))) return rc;
+    {   // the sloppy hop's per-site tables, built here, before the iterations are captured
+        Hop t{c, S_, gs_};
+        if ((rc = t.tables())) return rc;
+        links_s_ = t.links;
+        nbr_s_ = t.nbr;
+    }
     const size_t hb = c.half_bytes(P_);
     const size_t hs = c.half_bytes(S_);
     const size_t he = c.half_bytes(QCU_PRECISION_SINGLE);
@@ -341,7 +357,7 @@ int SchurSolve::enqueue_iteration() {
     const int* gate = &dsc_->gate;
     const int XP = QCU_PRECISION_SINGLE;
     Hop h64{c, P_, g_};
-    Hop hs{c, S_, gs_};
+    Hop hs{c, S_, gs_, links_s_, nbr_s_};
     // sloppy BiCGStab iteration
     if ((e = hs.launch(tmps, ps, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
     if ((e = hs.launch(vs, tmps, 1, EPI_SCHUR_R0, ps, r0s, k2, FIN_ALPHA, dsc_, dsc_->red[0], done))) return e;

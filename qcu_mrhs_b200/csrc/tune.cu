@@ -12,6 +12,7 @@ namespace qcub {
 bool hop_tc_supported(int nc, int m, int prec);
 bool hop16_supported(int nc, int m, int prec);
 bool hop16_pairs_supported(int nc, int m, int prec);
+bool hop_mmal_supported(int nc, int m, int prec);
 void set_hop_kind(int k);
 int hop_kind();
 
@@ -63,6 +64,7 @@ int auto_hop_kind(int nc, int m, int prec) {
     // measured on B200 (16^4 and 24^3x48, N = 3..8, m = 8..32): packed 16-bit arithmetic
     // wins for FP16/BF16 storage wherever it applies (two RHS per thread where that is
     // specialised), the per-(site, RHS) SIMT kernel everywhere else
+    if (hop_mmal_supported(nc, m, prec)) return QCU_HOP_MMA_LINK;
     if (hop16_pairs_supported(nc, m, prec)) return QCU_HOP_PACKED16_PAIRS;
     if (hop16_supported(nc, m, prec)) return QCU_HOP_PACKED16;
     return QCU_HOP_SIMT;
@@ -107,7 +109,8 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
     // the faster one, but its Schur and residual forms (two of the four hops of a solver
     // iteration) are slower than PACKED16_PAIRS's, and the solve with it is slower (B200,
     // 24^3x48, m = 12, FP16: 87.3 ms against 81.6 ms)
-    int kinds[5] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS};
+    int kinds[6] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
+                    QCU_HOP_MMA_LINK};
     int best = QCU_HOP_SIMT;
     float best_ms = 1e30f;
     for (int kind : kinds) {
@@ -115,6 +118,7 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         if (kind == QCU_HOP_TENSOR && !hop_tc_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16 && !hop16_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16_PAIRS && !hop16_pairs_supported(nc, m, prec)) continue;
+        if (kind == QCU_HOP_MMA_LINK && !hop_mmal_supported(nc, m, prec)) continue;
         set_hop_kind(kind);
         HopParams p{};
         p.in = in;

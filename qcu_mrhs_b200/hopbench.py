@@ -1,6 +1,6 @@
 """Micro-benchmark of the multi-RHS hop kernel through the C ABI (qcuDslashMrhs).
 
-  python -m qcu_mrhs_b200.hopbench --L 24 24 24 48 --nc 3 --m 12 --prec bf16 --reps 20
+  python -m qcu_mrhs_b200.hopbench --L 24 24 24 48 --nc 3 --m 12 --prec bf16 --reps 20 [--context]
 
 Prints one JSON line per precision: launch time (CUDA events on the launching
 stream, after warm-up), algorithmic GB/s and GFLOP/s.  Inputs are random device
@@ -16,7 +16,7 @@ import json
 
 PRECS = {"f64": 2, "f32": 1, "f16": 0, "bf16": 4}
 KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs",
-           "mma16", "packed16_pairs_blocked"]
+           "mma16", "mma_link", "packed16_pairs_blocked"]
 # the last entry is the two-RHS kernel on the site-blocked layout (qcuDslashMrhsSiteBlocked)
 BLOCKED = KERNELS.index("packed16_pairs_blocked")
 
@@ -29,7 +29,7 @@ def hop_flops(vh, nc, m):
     return vh * m * (128 * nc * nc + 56 * nc)
 
 
-def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
+def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0, context=False):
     import torch
 
     import qcu_mrhs_b200 as q
@@ -45,7 +45,23 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
     sp = ctypes.c_void_p(st.cuda_stream)
     lib = q.lib()
     q.check(lib.qcuSetHopKernel(q.HOP_PACKED16_PAIRS if kernel == BLOCKED else kernel))
-    hop = lib.qcuDslashMrhsSiteBlocked if kernel == BLOCKED else lib.qcuDslashMrhs
+    if context:
+        # the qcu.h context's hop (its gauge copy and, where the kernel reads them, the
+        # per-site tables): what the solver runs
+        grid = q.QcuGrid((ctypes.c_int * 4)(1, 1, 1, 1))
+        param = q.QcuParam((ctypes.c_int * 4)(*L))
+        lib.initGridSize(ctypes.byref(grid), ctypes.byref(param), nc, m, prec, prec)
+        q.check()
+        lib.loadQcuGauge(g.data_ptr(), prec)
+        lib.getDslash(0, 1.0)
+        o = q.default_options()
+        o.t_boundary = t_sign
+        q.check(lib.qcuSetSolverOptions(ctypes.byref(o)))
+
+        def hop(out, inp, gp, Lc_, nc_, m_, parity, dagger, ts, pr, stream):
+            return lib.qcuDslashMrhsContext(out, inp, parity, dagger, pr, stream)
+    else:
+        hop = lib.qcuDslashMrhsSiteBlocked if kernel == BLOCKED else lib.qcuDslashMrhs
     bufs = (a, b)
     for i in range(warmup):
         q.check(hop(bufs[(i + 1) & 1].data_ptr(), bufs[i & 1].data_ptr(), g.data_ptr(), Lc, nc, m,
@@ -61,7 +77,9 @@ def run(L, nc, m, prec_name, reps=20, warmup=3, t_sign=-1.0, kernel=0):
     dur = e0.elapsed_time(e1) / 1e3 / reps
     s = q.PREC_BYTES[prec]
     q.check(lib.qcuSetHopKernel(0))
-    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "kernel": KERNELS[kernel],
+    if context:
+        lib.finalizeQcu()
+    return {"L": list(L), "nc": nc, "m": m, "prec": prec_name, "kernel": KERNELS[kernel], "context": context,
             "launch_us": dur * 1e6,
             "GBps": hop_bytes(vh, nc, m, s) / dur / 1e9, "GFLOPs": hop_flops(vh, nc, m) / dur / 1e9,
             "algorithmic_bytes": hop_bytes(vh, nc, m, s)}
@@ -76,12 +94,14 @@ def main():
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--kernel", nargs="+", default=["auto"], choices=KERNELS)
+    ap.add_argument("--context", action="store_true",
+                    help="time qcuDslashMrhsContext (the context's hop, with its per-site tables)")
     args = ap.parse_args()
     for kname in args.kernel:
         kern = KERNELS.index(kname)
         for p in args.prec:
-            print(json.dumps(run(tuple(args.L), args.nc, args.m, p, args.reps, args.warmup, kernel=kern)),
-                  flush=True)
+            print(json.dumps(run(tuple(args.L), args.nc, args.m, p, args.reps, args.warmup, kernel=kern,
+                                 context=args.context)), flush=True)
 
 
 if __name__ == "__main__":

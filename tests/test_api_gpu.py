@@ -87,6 +87,88 @@ def test_mat_qcu_half_precision_dslash(oracle_lib):
     assert rel_err(got, oracle_lib.mat(psi, gauge, L, kappa)) <= 3e-3
 
 
+def _round(arr, prec):
+    """Round a complex array to a 16-bit storage format and back (torch on CPU)."""
+    import torch
+    dt = {q.HALF: torch.float16, q.BF16: torch.bfloat16}[prec]
+    a = np.ascontiguousarray(arr, dtype=np.complex128)
+    t = torch.from_numpy(a.view(np.float64).reshape(a.shape + (2,)).copy()).to(dt).to(torch.float64).numpy()
+    return t[..., 0] + 1j * t[..., 1]
+
+
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16])
+@pytest.mark.parametrize("t_boundary", [1.0, -1.0])
+@pytest.mark.parametrize("m", [4, 12, 7])
+def test_start_dslash_and_mat_low_precision_tables(oracle_lib, prec, t_boundary, m):
+    """16-bit start_dslash and mat_Qcu on a context: with the automatic kernel choice the hop
+    is the link-operand tensor-core kernel, which on a context reads the per-site neighbour
+    table and hop-link array (t-boundary sign folded in) instead of recomputing them.  Both
+    parities, dagger, both t boundaries, against the oracle on the same rounded inputs."""
+    L, nc, kappa = (8, 4, 4, 6), 3, 0.11
+    tol = {q.HALF: 2e-3, q.BF16: 1.5e-2}[prec]
+    gauge, dg = _setup(L, nc, m, kappa, 21, dslash_prec=prec)
+    o = q.default_options()
+    o.t_boundary = t_boundary
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    vh = F.half_volume(L)
+    gr = _round(gauge, prec)
+    psi = F.gaussian_fermions(L, nc, m, 22, parities=1)[:, 0]
+    ins = [to_dev(psi[j]) for j in range(m)]
+    for dagger in (0, 1):
+        for parity in (0, 1):
+            outs = [empty_dev((vh, 4, nc)) for _ in range(m)]
+            for j in range(m):
+                q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+            q.lib().start_dslash(parity, dagger)
+            q.check()
+            got = np.stack([from_dev(x) for x in outs])
+            ref = F.from_mrhs(oracle_lib.hop(_round(F.to_mrhs(psi), prec), gr, L, parity, bool(dagger), t_boundary))
+            assert rel_err(got, ref) <= tol
+    full = F.gaussian_fermions(L, nc, m, 23)
+    fins = [to_dev(full[j]) for j in range(m)]
+    for dagger in (0, 1):
+        outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+        for j in range(m):
+            q.lib().pushBackFermions(outs[j].data_ptr(), fins[j].data_ptr())
+        q.lib().mat_Qcu(dagger)
+        q.check()
+        got = np.stack([from_dev(x) for x in outs])
+        ref = oracle_lib.mat(full, gauge, L, kappa, bool(dagger), t_boundary)
+        assert rel_err(got, ref) <= tol
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16, q.DOUBLE])
+@pytest.mark.parametrize("m", [4, 8, 12, 16, 6])
+def test_context_hop(oracle_lib, prec, m):
+    """qcuDslashMrhsContext: the context's own hop (gauge copy, t boundary, and for FP16/BF16
+    the per-site tables; m = 4, 8, 12, 16 run the bulk-copy staged tensor-core kernel) on
+    caller gathered fields, both parities and dagger, against the oracle on the same
+    rounded inputs; the same call twice gives the same bits (the tables are reused)."""
+    L, nc, kappa = (8, 4, 4, 6), 3, 0.11
+    tol = {q.HALF: 2e-3, q.BF16: 1.5e-2, q.DOUBLE: 1e-13}[prec]
+    gauge, dg = _setup(L, nc, m, kappa, 31)
+    o = q.default_options()
+    o.t_boundary = -1.0
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    rnd = (lambda a: a) if prec == q.DOUBLE else (lambda a: _round(a, prec))
+    inp = F.to_mrhs(F.gaussian_fermions(L, nc, m, 32, parities=1)[:, 0])
+    d_in = to_dev(inp, prec)
+    for dagger in (0, 1):
+        for parity in (0, 1):
+            d_out = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuDslashMrhsContext(d_out.data_ptr(), d_in.data_ptr(), parity, dagger, prec, None))
+            sync()
+            ref = oracle_lib.hop(rnd(inp), rnd(gauge), L, parity, bool(dagger), -1.0)
+            got = from_dev(d_out)
+            assert rel_err(got, ref) <= tol
+            d_out2 = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuDslashMrhsContext(d_out2.data_ptr(), d_in.data_ptr(), parity, dagger, prec, None))
+            sync()
+            assert np.array_equal(got, from_dev(d_out2))
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
 _LAST = {"error": ""}
 
 
@@ -150,8 +232,8 @@ def test_mixed_precision_reaches_fp64_true_residual(oracle_lib, sloppy):
     assert np.allclose(true_rel, np.array(stats.true_residual[:m]), rtol=1e-2, atol=1e-15)
 
 
-@pytest.mark.parametrize("kind", [q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_PAIRS],
-                         ids=["packed16", "packed16_acc16", "packed16_pairs"])
+@pytest.mark.parametrize("kind", [q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_PAIRS, q.HOP_MMA_LINK],
+                         ids=["packed16", "packed16_acc16", "packed16_pairs", "mma_link"])
 @pytest.mark.parametrize("sloppy", [q.HALF, q.BF16])
 def test_mixed_precision_with_packed_hop(oracle_lib, sloppy, kind):
     """The packed 16-bit hop inside the mixed solver: its Schur epilogues and fused

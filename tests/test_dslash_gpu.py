@@ -98,8 +98,9 @@ def _acc16_factor(kind, prec):
 
 
 LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16,
-                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS, q.HOP_MMA16]
-LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs", "mma16"]
+                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS, q.HOP_MMA16, q.HOP_MMA_LINK]
+LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs", "mma16",
+            "mma_link"]
 
 
 @pytest.mark.parametrize("hop_kernel", LOWP_KERNELS, indirect=True, ids=LOWP_IDS)
@@ -122,8 +123,9 @@ def test_low_precision_hop(oracle_lib, prec, nc, m, hop_kernel):
 
 
 @pytest.mark.parametrize("hop_kernel", [q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16, q.HOP_PACKED16_STAGED,
-                                        q.HOP_PACKED16_PAIRS], indirect=True,
-                         ids=["tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs"])
+                                        q.HOP_PACKED16_PAIRS, q.HOP_MMA_LINK], indirect=True,
+                         ids=["tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs",
+                              "mma_link"])
 @pytest.mark.parametrize("prec", [q.HALF, q.BF16])
 @pytest.mark.parametrize("L", [(2, 2, 2, 2), (6, 2, 4, 2), (4, 4, 4, 6), (8, 8, 8, 10)])
 def test_low_precision_hop_shapes_and_epilogues(oracle_lib, prec, L, hop_kernel):
@@ -207,10 +209,10 @@ def test_autotuner_records_a_valid_choice(tmp_path, monkeypatch):
     for prec in (q.DOUBLE, q.BF16):
         k = q.lib().qcuTuneHop(q.lattice(L), 3, 12, prec, None)
         assert k in (q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_PAIRS,
-                     q.HOP_MMA16), q.last_error()
+                     q.HOP_MMA16, q.HOP_MMA_LINK), q.last_error()
         assert q.lib().qcuGetTunedHop(3, 12, prec) == k
         if prec == q.DOUBLE:
-            assert k not in (q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_PAIRS, q.HOP_MMA16)
+            assert k not in (q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_PAIRS, q.HOP_MMA16, q.HOP_MMA_LINK)
     assert q.lib().qcuTuneHop(q.lattice((7, 4, 4, 4)), 3, 12, q.DOUBLE, None) < 0
 
 
