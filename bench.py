@@ -52,6 +52,16 @@ CHECK_INTERVAL = 16
 # gpu__time_duration from one ncu capture of the kernel at this size, plain epilogue);
 # keyed by (storage precision, kernel)
 MEASURED_TRAFFIC = {("f16", "packed16_pairs"): 490.7e6, ("f16", "packed16"): 530.2e6, ("f16", "simt"): 610.6e6}
+# arithmetic of each 16-bit hop kernel
+DTYPE_DETAIL = {
+    "mma_link": "FP16 storage; spin projection in FP16 (one rounding), link products and the sum of the 8 hops "
+                "in FP32 on the tensor cores (mma.sync m16n8k16, FP32 accumulate)",
+    "packed16_pairs": "FP16 storage; projection and the 3-term colour sums of each link product in packed FP16, "
+                      "the 8 hops summed in FP32",
+    "packed16": "FP16 storage; projection and the 3-term colour sums of each link product in packed FP16, "
+                "the 8 hops summed in FP32",
+    "simt": "FP16 storage, FP32 arithmetic",
+}
 
 
 def peaks():
@@ -148,6 +158,32 @@ def make_fields(rank):
     return gauge, src
 
 
+def cpu_solve_timing(bm, gauge, plain_iters, repeats=3, n_hi=4):
+    """Time-to-solve of the CPU restatement (FP64 policy-1 Schur BiCGStab, all host threads) on
+    a bounded sample: `repeats` runs of setup + 1 iteration and `repeats` runs of setup +
+    n_hi iterations; per-iteration time from the difference of the medians, extrapolated to
+    the GPU plain solve's iteration count.  Returns value, per-iteration time, spread, sample."""
+    from oracle import oracle as O
+
+    def one(n_it):
+        t0 = time.perf_counter()
+        O.bicgstab(bm, gauge, L, KAPPA, n_it, TOL, t_sign=T_BOUNDARY)
+        return time.perf_counter() - t0
+    one(1)   # warm-up (page-in, thread pool)
+    t1 = [one(1) for _ in range(repeats)]
+    th = [one(n_hi) for _ in range(repeats)]
+    m1, mh = statistics.median(t1), statistics.median(th)
+    t_iter = max((mh - m1) / (n_hi - 1), 1e-9)
+    t_setup = max(m1 - t_iter, 0.0)
+    value = t_setup + t_iter * plain_iters
+    spread = {"setup_plus_1_iteration_s": [min(t1), m1, max(t1)],
+              f"setup_plus_{n_hi}_iterations_s": [min(th), mh, max(th)]}
+    sample = (f"{repeats} x (setup + 1 iteration) and {repeats} x (setup + {n_hi} iterations) of the FP64 "
+              f"policy-1 BiCGStab on the full workload ({sum(t1) + sum(th):.1f} s of CPU work); per-iteration "
+              f"time from the medians, extrapolated to {plain_iters} iterations")
+    return value, t_iter, spread, sample
+
+
 def run_reference(args, world, rank):
     """CPU reference leg: the FP64 policy-1 Schur BiCGStab of the CPU restatement
     (the reference has no CPU implementation of its own), all host threads."""
@@ -163,30 +199,16 @@ def run_reference(args, world, rank):
     b = b.numpy()
     bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
     del b
-    iters = PLAIN_ITERS or 1
-    # one step: setup + one BiCGStab iteration (bounded sample); per-iteration time
-    # from the difference of one- and two-iteration runs
-    def one(n_it):
-        t0 = time.perf_counter()
-        O.bicgstab(bm, gauge, L, KAPPA, n_it, TOL, t_sign=T_BOUNDARY)
-        return time.perf_counter() - t0
-    for _ in range(args.warmup):
-        one(1)
-    t1 = [one(1) for _ in range(args.steps)]
-    t2 = one(2)
-    t_iter = max(t2 - statistics.median(t1), 1e-9)
-    t_setup = max(statistics.median(t1) - t_iter, 0.0)
-    value = t_setup + t_iter * iters
+    value, t_iter, spread, sample = cpu_solve_timing(bm, gauge, PLAIN_ITERS or 1,
+                                                     repeats=max(3, min(args.steps, 5)))
     line = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(t1) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded smoothed SU(3) links, unit complex Gaussian sources",
         "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} x (setup + 1 iteration) and 1 x (setup + 2 iterations) of the "
-                                   f"FP64 policy-1 BiCGStab on the full workload; time-to-solve extrapolated "
-                                   f"as setup + per-iteration time x {iters} iterations"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample,
+                         "per_iteration_s": t_iter, "spread": spread},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -230,7 +252,9 @@ def main():
 
     grid = q.QcuGrid((ctypes.c_int * 4)(1, 1, 1, 1))
     param = q.QcuParam((ctypes.c_int * 4)(*L))
-    lib.initGridSize(ctypes.byref(grid), ctypes.byref(param), NC, M, q.DOUBLE, q.BF16)
+    # dslash precision FP64: mat_Qcu (the independent residual check below) runs in FP64;
+    # the solvers' precisions are set by the solver options
+    lib.initGridSize(ctypes.byref(grid), ctypes.byref(param), NC, M, q.DOUBLE, q.DOUBLE)
     q.check()
     lib.loadQcuGauge(d_gauge.data_ptr(), q.DOUBLE)
     lib.getDslash(0, 1.0 / (2 * KAPPA) - 4.0)
@@ -252,8 +276,8 @@ def main():
     names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16", 9: "mma_link"}
     for name, prec in (("f64", q.DOUBLE), ("f16", q.HALF), ("bf16", q.BF16)):
         if args.static_kernels:
-            k = lib.qcuGetTunedHop(NC, M, prec)   # 0 (nothing recorded): the static rule applies
-            tuned[name] = names.get(k, "static rule")
+            k = lib.qcuGetAutoHop(NC, M, prec)    # the static rule (nothing recorded)
+            tuned[name] = names.get(k, str(k))
             continue
         k = lib.qcuTuneHop(q.lattice(L), NC, M, prec, None)
         if k < 0:
@@ -269,6 +293,21 @@ def main():
         if st not in (q.SUCCESS,):
             raise RuntimeError(f"qcuInvert failed: {q.last_error()}")
         return q.solve_stats()
+
+    d_mx = [torch.empty_like(d_src[0]) for _ in range(M)]
+
+    def true_residual(xs):
+        """max_j ||b_j - M x_j|| / ||b_j|| of the full system, recomputed in FP64 through
+        mat_Qcu (independent of the solver's own statistics), outside any timed region."""
+        for j in range(M):
+            lib.pushBackFermions(d_mx[j].data_ptr(), xs[j].data_ptr())
+        lib.mat_Qcu(0)
+        q.check()
+        worst = 0.0
+        for j in range(M):
+            worst = max(worst, float(torch.linalg.vector_norm(d_src[j] - d_mx[j]) /
+                                     torch.linalg.vector_norm(d_src[j])))
+        return worst
 
     def barrier():
         if world > 1:
@@ -297,6 +336,7 @@ def main():
     t_mixed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps)
     clk = clocks.stop()
     reliable = stats.reliable_updates
+    check_mixed = true_residual(d_x)
 
     # ---- the same solve with BF16 storage ----
     set_opts(q.SOLVER_MIXED, q.BF16)
@@ -307,6 +347,7 @@ def main():
     ev1.record()
     torch.cuda.synchronize()
     t_bf16 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    check_bf16 = true_residual(d_x)
 
     # ---- plain FP64 BiCGStab (same fields, same GPU) ----
     set_opts(q.SOLVER_FUSED)
@@ -322,6 +363,7 @@ def main():
     t_plain = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     it_plain = stats_plain.iterations
     rel_plain = max(stats_plain.true_residual[:M])
+    check_plain = true_residual(d_x)
 
     # ---- dslash roofline: the FP16 hop (dominant kernel of the solve), BF16 and FP64 beside it;
     #      dslash error of each storage precision against the FP64 hop (which matches the
@@ -416,20 +458,26 @@ def main():
             "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f16",
-            "dtype_detail": "FP16 storage, FP32 arithmetic, FP64 reductions, reliable updates and solution",
+            "dtype_detail": DTYPE_DETAIL.get(tuned["f16"], "FP16 storage, FP32 arithmetic") +
+                            "; FP64 reductions, reliable updates and solution",
             "data": "synthetic: seeded smoothed SU(3) links exp(i 0.3 H), unit complex Gaussian sources",
             "config": {"workload": WORKLOAD, "lattice": list(L), "n_color": NC, "m_rhs": M, "kappa": KAPPA,
                        "tol": TOL, "l2": "inputs larger than L2 (each hop reads 478 MB in BF16, 1.9 GB in FP64)",
                        "replicas": world, "reliable_delta_quorum": RELIABLE, "check_interval": CHECK_INTERVAL,
                        "hop_kernels": tuned},
             "solves_per_s_all_ranks": world / t_mixed,
-            "mixed": {"iterations": it_mixed[-1], "reliable_updates": reliable, "true_residual_max": max(rel_mixed)},
+            "mixed": {"iterations": it_mixed[-1], "reliable_updates": reliable, "true_residual_max": max(rel_mixed),
+                      "true_residual_check": check_mixed},
             "mixed_bf16": {"value": t_bf16, "unit": "s", "iterations": stats_bf.iterations,
                            "reliable_updates": stats_bf.reliable_updates,
                            "true_residual_max": max(stats_bf.true_residual[:M]),
+                           "true_residual_check": check_bf16,
                            "speedup_vs_plain": t_plain / t_bf16},
+            "true_residual_check": "max_j ||b_j - M x_j|| / ||b_j||, recomputed in FP64 with mat_Qcu from "
+                                   "the returned solutions, outside the timed region",
             "dslash_rel_err_vs_fp64": dslash_err,
             "plain_fp64": {"value": t_plain, "unit": "s", "iterations": it_plain, "true_residual_max": rel_plain,
+                           "true_residual_check": check_plain,
                            "speedup_mixed_vs_plain": t_plain / t_mixed},
             "roofline": roof["f16"],
             "roofline_bf16_hop": roof["bf16"],
@@ -447,9 +495,8 @@ def main():
 
 
 def cpu_baseline(d_gauge, d_src, plain_iters):
-    """CPU restatement (FP64 policy-1 BiCGStab), all host threads, bounded sample:
-    setup + 1 and setup + 2 iterations on the same fields; time-to-solve extrapolated
-    with the GPU plain solve's iteration count."""
+    """CPU restatement (FP64 policy-1 BiCGStab), all host threads, bounded sample on the same
+    fields (cpu_solve_timing)."""
     from oracle import oracle as O
     from qcu_mrhs_b200 import fields as F
     O.build()
@@ -461,19 +508,9 @@ def cpu_baseline(d_gauge, d_src, plain_iters):
     b = b[..., 0] + 1j * b[..., 1]                      # [m][2][vh][4][nc]
     bm = np.stack([F.to_mrhs(b[:, 0]), F.to_mrhs(b[:, 1])])
     del b, g
-
-    def one(n_it):
-        t0 = time.perf_counter()
-        O.bicgstab(bm, gauge, L, KAPPA, n_it, TOL, t_sign=T_BOUNDARY)
-        return time.perf_counter() - t0
-    t1 = one(1)
-    t2 = one(2)
-    t_iter = max(t2 - t1, 1e-9)
-    t_setup = max(t1 - t_iter, 0.0)
-    return {"value": t_setup + t_iter * plain_iters, "unit": "s", "cores": threads, "kind": "port",
-            "sample": f"setup+1 and setup+2 iterations of the FP64 policy-1 BiCGStab on the full workload "
-                      f"({t1 + t2:.1f} s of CPU work); extrapolated to {plain_iters} iterations",
-            "per_iteration_s": t_iter}
+    value, t_iter, spread, sample = cpu_solve_timing(bm, gauge, plain_iters)
+    return {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample,
+            "per_iteration_s": t_iter, "spread": spread}
 
 
 if __name__ == "__main__":

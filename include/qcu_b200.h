@@ -271,9 +271,10 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *   SIMT     one thread per (site, RHS), all colours in registers;
  *   SIMT_CS  one thread per (site, RHS, colour): fewer registers (FP64, large N),
  *            needs n_color * m_rhs <= 256 (else SIMT);
- *   TENSOR   FP16/BF16 storage on the tcgen05 tensor cores with TMEM accumulators and
- *            bulk-copy (TMA) staged neighbour spinors, for 2 <= n_color <= 4 and
- *            m_rhs <= 32 (else SIMT);
+ *   TENSOR   FP16/BF16 storage on the tcgen05 tensor cores with TMEM accumulators, the
+ *            MMA operands (projected neighbour spinors, embedded links) written to shared
+ *            memory by the CTA's threads, for 2 <= n_color <= 4 and m_rhs <= 32 (else
+ *            SIMT);
  *   PACKED16 FP16/BF16 storage, projection and link products in packed 16-bit complex
  *            arithmetic, the 8 hops summed in FP32; 2 <= n_color <= 4, m_rhs >= 2
  *            (else SIMT);
@@ -293,8 +294,12 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *   MMA_LINK FP16/BF16, 2 <= n_color <= 4, any m_rhs: one warp per (site, up to 16 RHS),
  *            the links as the A operand of mma.sync m16n8k16 and the projected neighbour
  *            half spinors (columns = RHS x half spinor) as B; the forward and backward hop
- *            of a direction are one MMA per 4 RHS, link products and all sums in FP32, the
- *            spin projection the only 16-bit arithmetic; else as AUTO;
+ *            of a direction are one MMA per 4 RHS, link products and the sum of the 8 hops
+ *            in FP32, the spin projection the only 16-bit arithmetic.  On a context (the
+ *            solvers, start_dslash, mat_Qcu, qcuDslashMrhsContext) it reads a per-site
+ *            neighbour table and hop-link array, and for m_rhs = 4, 8, 12, 16 stages the
+ *            neighbour and link blocks in shared memory with bulk asynchronous copies
+ *            (whole rows of the half lattice per block where Lx <= 32); else as AUTO;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
  *            (n_color, m_rhs, precision), else PACKED16_PAIRS, PACKED16 or SIMT,
  *            the first that applies. */
@@ -319,6 +324,8 @@ int qcuGetHopKernel(void);
 int qcuTuneHop(const int L[4], int n_color, int m_rhs, int precision, void *stream);
 /* Recorded choice for AUTO (0 = none recorded). */
 int qcuGetTunedHop(int n_color, int m_rhs, int precision);
+/* The kind AUTO runs for a shape: the recorded choice, else the static rule. */
+int qcuGetAutoHop(int n_color, int m_rhs, int precision);
 
 /* Nonzero if a kernel on the current device gave up a bounded wait (its results are then
  * invalid); synchronises the device.  clear != 0 resets the flag. */
@@ -326,6 +333,22 @@ int qcuGetKernelError(int clear);
 
 /* Device synchronisation helper for bindings that have no CUDA runtime of their own. */
 int qcuDeviceSynchronize(void);
+
+/* Arithmetic peak microbenchmarks: the compute ceilings of the hop kernels.  kind:
+ *   DFMA  FP64 fused multiply-add on the CUDA cores
+ *   FFMA  FP32 fused multiply-add on the CUDA cores
+ *   DMMA  FP64 warp MMA (mma.sync m8n8k4, FP64 accumulation)
+ *   HMMA  FP16 warp MMA (mma.sync m16n8k16, FP32 accumulation: the link-operand hop's MMA)
+ *   BMMA  BF16 warp MMA (same shape)
+ * Launches 4 blocks of 256 threads per SM, each thread (FMA) or warp (MMA) issuing `iters`
+ * rounds of 8 independent operations, times the second of two launches with CUDA events on
+ * `stream` and writes FLOP/s to *flops. */
+#define QCU_PEAK_DFMA 1
+#define QCU_PEAK_FFMA 2
+#define QCU_PEAK_DMMA 3
+#define QCU_PEAK_HMMA 4
+#define QCU_PEAK_BMMA 5
+int qcuPeakRate(int kind, int iters, double *flops, void *stream);
 
 #ifdef __cplusplus
 }

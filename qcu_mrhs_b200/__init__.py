@@ -25,6 +25,7 @@ SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND, SOLVER_CGNR = 0, 1, 2, 3, 4
 (HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16, HOP_PACKED16_STAGED,
  HOP_PACKED16_PAIRS, HOP_MMA16, HOP_MMA_LINK) = range(10)
+PEAK_DFMA, PEAK_FFMA, PEAK_DMMA, PEAK_HMMA, PEAK_BMMA = 1, 2, 3, 4, 5
 MAX_RHS = 64
 
 
@@ -140,7 +141,9 @@ _SIGNATURES = {
     "qcuGetKernelError": (_i, [_i]),
     "qcuTuneHop": (_i, [_ip, _i, _i, _i, _vp]),
     "qcuGetTunedHop": (_i, [_i, _i, _i]),
+    "qcuGetAutoHop": (_i, [_i, _i, _i]),
     "qcuDeviceSynchronize": (_i, []),
+    "qcuPeakRate": (_i, [_i, _i, ctypes.POINTER(_d), _vp]),
     "qcuPrecondCreate": (_i, [ctypes.POINTER(_vp), _ip, _i, _i, _i, _i, _d]),
     "qcuPrecondDestroy": (_i, [_vp]),
     "qcuPrecondNumWeights": (_i64, [_vp]),

@@ -1,146 +1,13 @@
-// dslash_mmal.cu -- multi-RHS hop term for FP16 / BF16 storage on the warp-level tensor-core
-// MMA (mma.sync m16n8k16, 16-bit operands, FP32 accumulation) with the LINKS as the A operand
-// and the projected neighbour spinors as the B operand.
-//
-// Same operator, layouts and epilogues as dslash_impl.cuh (reference
-// include/kernel/su_n_m_rhs_dslash.cuh:92-105, complex_matmul.cuh:16-600, whose solver hop
-// also runs the link products through tensor-core tiles).
-//
-// Work unit: one warp per (half-site, chunk of up to 16 RHS); inside it, groups of 4 RHS.
-// For direction mu, with the forward hop matrix W_f = U_mu(x) (t-boundary sign folded in)
-// and the backward one W_b = U_mu(x - mu)^dag, one real MMA per group of 4 RHS does both hops:
-//   K (16)   8 complex slots as (re, im) pairs: slot c = forward colour c, slot 4 + c =
-//            backward colour c (N <= 4; the rest zero)
-//   B (16x8) column j = (RHS j/2 of the group, half spinor j%2): the projected forward and
-//            backward neighbour half spinors h_f, h_b (lane 4g+t holds column g, colour t)
-//   A (16x16) rows 0..2N-1, "sum" rows (c', re/im):  [emb(W_f)      | emb(W_b)]
-//            rows 8..8+2N-1, "diff" rows (c', re/im): [emb(phi W_f) | emb(-phi W_b)]
-//   D        sum rows: W_f h_f + W_b h_b, which spins 0 and 1 take as they are (column
-//            h = 0 and 1); diff rows: phi (W_f h_f - W_b h_b), phi = the lower-spin phase of
-//            the forward projector (the backward projector's is -phi)
-// emb(W) is the real embedding [[W.re, -W.im], [W.im, W.re]] of each complex entry.  The
-// lower spins take the diff rows with a direction-dependent column (the x and y projectors
-// exchange the half spinors) and sign (y and z flip spin 3), so every direction has its
-// own D tile (4 FP32 per lane) and the tiles are added at the end, in FP32:
-//   spin0 = sum_mu D_mu[sum, h0]          spin1 = sum_mu D_mu[sum, h1]
-//   spin2 = D_x[diff,h1] + D_y[diff,h1] + D_z[diff,h0] + D_t[diff,h0]
-//   spin3 = D_x[diff,h0] - D_y[diff,h0] - D_z[diff,h1] + D_t[diff,h1]
-// So the link products and all sums are FP32; the only 16-bit arithmetic is the spin
-// projection (one rounding of p_a + kappa p_b, kappa in {+-1, +-i}) and the final store.
-//
-// Fragment layouts (PTX ISA, mma.m16n8k16, 16-bit A/B): lane = 4 g + t holds
-//   A: a0 = (row g, k 2t..2t+1), a1 = (row g+8, k 2t..), a2 = (row g, k 2t+8..), a3 = (row g+8, k 2t+8..)
-//   B: b0 = (k 2t..2t+1, col g), b1 = (k 2t+8..2t+9, col g)
-//   D: d0, d1 = (row g, col 2t..2t+1), d2, d3 = (row g+8, col 2t..2t+1)
-// so lane (g, t) builds its A words from the link elements W_f[g/2][t], W_b[g/2][t], loads
-// the neighbour words of (half spinor g%2, colour t, RHS g/2) and ends with component g%2
-// (re/im) of the four output spins of (colour g/2, RHS t).  Lanes g and g^1 (lane ^ 4)
-// exchange halves so that each stores two whole complex words.  Lanes outside the colour
-// range load clamped (finite) words that meet zero A entries, and store nothing.
-//
-// For 5 <= N <= 8 the sum and diff rows are two M tiles and the forward and backward
-// colours two K steps (4 MMAs per direction and group); the sum tile is shared by the
-// directions, the diff tiles are per direction.
-#include <type_traits>
+// dslash_mmal.cu -- the link-operand tensor-core hop for N <= 4 (fragment scheme in
+// dslash_mmal.cuh) and the public entry points of the link-operand hop.
+#include <algorithm>
+#include <cstdlib>
 
-#include "dslash.h"
-#include "dslash_impl.cuh"
-#include "workspace.h"
+#include "dslash_mmal.cuh"
 
 namespace qcub {
 
-int* device_error_flag();   // runtime.cu: per-device flag, nonzero after a timed-out wait
-
 namespace {
-
-constexpr int kLThreads = 256;
-constexpr int kLWarps = kLThreads / 32;
-constexpr int kLMaxChunkRhs = 16;   // RHS per work unit (4 groups of 4)
-
-template <typename S> struct LMma;
-template <> struct LMma<__half> {
-    static constexpr uint32_t kOne = 0x3C00u;
-    __device__ static void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
-                               float c1, float c2, float c3) {
-        asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%10,%11,%12,%13};"
-            : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
-            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
-    }
-    __device__ static uint32_t fma(uint32_t a, uint32_t b, uint32_t c) {
-        const __half2 r = __hfma2(*reinterpret_cast<const __half2*>(&a), *reinterpret_cast<const __half2*>(&b),
-                                  *reinterpret_cast<const __half2*>(&c));
-        return *reinterpret_cast<const uint32_t*>(&r);
-    }
-    __device__ static uint32_t pack(float lo, float hi) {
-        const __half2 r = __floats2half2_rn(lo, hi);
-        return *reinterpret_cast<const uint32_t*>(&r);
-    }
-    __device__ static float2 unpack(uint32_t u) { return __half22float2(*reinterpret_cast<const __half2*>(&u)); }
-};
-template <> struct LMma<__nv_bfloat16> {
-    static constexpr uint32_t kOne = 0x3F80u;
-    __device__ static void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
-                               float c1, float c2, float c3) {
-        asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%10,%11,%12,%13};"
-            : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
-            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
-    }
-    __device__ static uint32_t fma(uint32_t a, uint32_t b, uint32_t c) {
-        const __nv_bfloat162 r = __hfma2(*reinterpret_cast<const __nv_bfloat162*>(&a),
-                                         *reinterpret_cast<const __nv_bfloat162*>(&b),
-                                         *reinterpret_cast<const __nv_bfloat162*>(&c));
-        return *reinterpret_cast<const uint32_t*>(&r);
-    }
-    __device__ static uint32_t pack(float lo, float hi) {
-        const __nv_bfloat162 r = __floats2bfloat162_rn(lo, hi);
-        return *reinterpret_cast<const uint32_t*>(&r);
-    }
-    __device__ static float2 unpack(uint32_t u) {
-        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u));
-    }
-};
-
-// packed pair of +-1 in the 16-bit format (lo in the low half)
-template <typename S>
-__host__ __device__ constexpr uint32_t unit_pair(int lo, int hi) {
-    return (LMma<S>::kOne | (lo < 0 ? 0x8000u : 0u)) | ((LMma<S>::kOne | (hi < 0 ? 0x8000u : 0u)) << 16);
-}
-__device__ __forceinline__ uint32_t swap_halves(uint32_t u) { return __byte_perm(u, 0, 0x1032); }
-
-// phase codes: 0 = +1, 1 = -1, 2 = +i, 3 = -i
-__host__ __device__ constexpr int lphase(int s, bool imag) { return (imag ? 2 : 0) + (s > 0 ? 0 : 1); }
-// lower-spin phase of spin 2 for direction MU and projector sign SG (spin2 += C2 (W h)_{P2});
-// spin 3 takes +-C2 (W h)_{P3} (the tables of dslash_impl.cuh)
-template <int MU, int SG>
-struct LRecon {
-    static constexpr int C2 = MU == 0 ? lphase(-SG, true) : MU == 1 ? lphase(SG, false)
-                            : MU == 2 ? lphase(-SG, true) : lphase(SG, false);
-};
-// emb(c W) from e = emb(W) of this lane's row (re rows: (W.re, -W.im), im rows: (W.im, W.re)):
-//   emb(-W) = e ^ sign bits; emb(iW) = swap(e) ^ high sign; emb(-iW) = swap(e) ^ low sign
-template <int C>
-__device__ __forceinline__ uint32_t emb_phase(uint32_t e) {
-    if (C == 0) return e;
-    if (C == 1) return e ^ 0x80008000u;
-    if (C == 2) return swap_halves(e) ^ 0x80000000u;
-    return swap_halves(e) ^ 0x00008000u;
-}
-
-// Projection of one neighbour word pair for lane column h = g % 2 (see the kernel comment):
-//   MU 0: h = p_h + s i p_{3-h}      MU 1: h = p_h + (h ? s : -s) p_{3-h}
-//   MU 2: h = p_h + (h ? -s : s) i p_{2+h}      MU 3: h = p_h + s p_{2+h}
-// as one packed FMA p + mult * q (q swapped for the i cases); `lm` is the lane's multiplier
-// for MU 1 / MU 2 (it depends on h).
-template <typename S, int MU, int SG>
-__device__ __forceinline__ uint32_t lproject(uint32_t pw, uint32_t qw, uint32_t lm) {
-    using M = LMma<S>;
-    if (MU == 0) return M::fma(swap_halves(qw), unit_pair<S>(-SG, SG), pw);
-    if (MU == 1) return M::fma(qw, lm, pw);
-    if (MU == 2) return M::fma(swap_halves(qw), lm, pw);
-    return M::fma(qw, unit_pair<S>(SG, SG), pw);
-}
 
 // One direction for all groups of the work unit: the four neighbour words of every group
 // are requested first, then each group's two projections and one MMA that adds the forward
@@ -171,40 +38,6 @@ __device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __r
         const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
         M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
     }
-}
-
-// A fragment of direction MU.  Rows are ordered (re/im, sum/diff, colour): lane (g, t) holds
-// rows g (re) and g + 8 (im) of class cls = g / 4 (0 sum, 1 diff) and colour g % 4, for
-// K slots t (forward colour t) and t + 4 (backward colour t).  wf = W_f[g%4][t] (t-boundary
-// sign folded in), wb = W_b[g%4][t] = conj(U_b[t][g%4]); diff lanes take phi W_f and -phi W_b,
-// applied as a lane byte permute (psel: identity or half swap) and sign mask (pmf / pmb).
-// emb re row: (w.re, -w.im) = w ^ high sign; im row: (w.im, w.re) = swap(w).
-__device__ __forceinline__ void mmal_a(uint32_t (&A)[4], uint32_t wf, uint32_t wb, uint32_t okm, uint32_t psel,
-                                       uint32_t pmf, uint32_t pmb) {
-    const uint32_t ff = (__byte_perm(wf, 0, psel) ^ pmf) & okm;
-    const uint32_t fb = (__byte_perm(wb, 0, psel) ^ pmb) & okm;
-    A[0] = ff ^ 0x80000000u;
-    A[1] = swap_halves(ff);
-    A[2] = fb ^ 0x80000000u;
-    A[3] = swap_halves(fb);
-}
-
-// lane phase constants of the diff rows for a direction whose forward lower-spin phase has
-// code C (0 = +1, 1 = -1, 2 = +i, 3 = -i): phi w = perm(w, sel) ^ mask (i w = swap(w) ^ low sign)
-struct LPhase {
-    uint32_t sel, mf, mb;
-};
-template <int C>
-__device__ __forceinline__ LPhase lphase_lane(bool diff) {
-    LPhase r;
-    constexpr bool imag = C >= 2;
-    constexpr uint32_t mpos = imag ? 0x00008000u : 0u;              // +1 or +i
-    constexpr uint32_t mneg = imag ? 0x80000000u : 0x80008000u;     // -1 or -i
-    constexpr bool neg = (C & 1) != 0;
-    r.sel = (diff && imag) ? 0x1032u : 0x3210u;
-    r.mf = diff ? (neg ? mneg : mpos) : 0u;
-    r.mb = diff ? (neg ? mpos : mneg) : 0u;   // backward: -phi
-    return r;
 }
 
 // Resident blocks per SM asked of the register allocator: 3 (80 registers) for the forms
@@ -479,18 +312,24 @@ constexpr int kTBarBytes = 64;   // mbarriers of the block (kTWarps x kTStages x
 
 __device__ __forceinline__ uint32_t lsmem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
+__device__ __forceinline__ bool lbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: the clock is read only once the first try has failed (in the common case
+// the copies have landed and the wait costs one try)
 __device__ __forceinline__ bool lbar_wait(uint32_t bar, uint32_t parity) {
+    if (lbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (ok) return true;
+        if (lbar_try(bar, parity)) return true;
         if (clock64() - t0 > (1ll << 31)) return false;   // about a second
     }
 }
@@ -582,28 +421,26 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
     const uint32_t nw = gridDim.x * kTWarps;
     // copy the blocks of `site` into stage k (lane 0 arms the barrier with the byte count;
     // lanes 0-7 take neighbour nbi, lane 8 the links, lanes 9-10 the epilogue blocks)
+    // lane roles of a copy round, fixed for the kernel: source base and per-site stride,
+    // destination offset in the stage, bytes; the copy itself is predicated, not branched
+    const bool cp_nb = lane < 8, cp_on = lane < 9 + NX;
+    const unsigned char* cp_base = lane == 8 ? links + (size_t)parity * vh * (LW * 4)
+                                 : (lane == 9 ? xv : (lane == 10 ? yv : in));
+    const uint32_t cp_stride = lane == 8 ? LW * 4 : SBY;
+    const uint32_t cp_dst = lane < 8 ? lane * SBY : (lane == 8 ? 8 * SBY : 8 * SBY + LW * 4 + (lane - 9) * SBY);
+    const uint32_t cp_bytes = lane == 8 ? LW * 4 : SBY;
+    const uint32_t stage_s = lsmem(stage);
     auto issue = [&](int k, uint32_t site, uint32_t nbi) {
         const uint32_t bar = bar0 + 8 * k;
         if (lane == 0) asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TX) : "memory");
         __syncwarp();
-        const unsigned char* src = nullptr;
-        uint32_t dst = lsmem(stage + k * STW), bytes = SBY;
-        if (lane < 8) {
-            src = in + (size_t)nbi * SBY;
-            dst += lane * SBY;
-        } else if (lane == 8) {
-            src = links + ((size_t)parity * vh + site) * (LW * 4);
-            dst += 8 * SBY;
-            bytes = LW * 4;
-        } else if (lane < 9 + NX) {
-            src = (lane == 9 ? xv : yv) + (size_t)site * SBY;
-            dst += 8 * SBY + LW * 4 + (lane - 9) * SBY;
-        }
-        if (src) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
-        }
+        const unsigned char* src = cp_base + (size_t)(cp_nb ? nbi : site) * cp_stride;
+        const uint32_t dst = stage_s + k * (STW * 4) + cp_dst;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %4, 0;\n\t"
+            "@p fence.proxy.async.shared::cta;\n\t"
+            "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n\t}"
+            ::"r"(dst), "l"(src), "r"(cp_bytes), "r"(bar), "r"((uint32_t)cp_on) : "memory");
     };
 
     float2 red[NTC][NVR];
@@ -674,11 +511,13 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
             ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
             ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
             ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
-            if (!sok) continue;
             if constexpr (EPI == EPI_PLAIN) {
-                out[ob + 4 * n] = M::pack(ov[0].x, ov[0].y);
-                out[ob + 4 * n + osn] = M::pack(ov[1].x, ov[1].y);
-            } else {
+                const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
+                if (sok) {
+                    out[ob + 4 * n] = w0;
+                    out[ob + 4 * n + osn] = w1;
+                }
+            } else if (sok) {
                 const float a = (float)p.a;
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
@@ -752,6 +591,274 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Asynchronous-copy variant of the staged kernel: the same stage layout, filled by the
+// lanes' own 16-byte asynchronous copies (cp.async.cg: global through L2 into shared memory)
+// instead of bulk copies.  Each lane gives its own addresses at no extra cost (a bulk copy
+// takes warp-uniform operands, so per-lane ones are issued one lane at a time), completion
+// is tracked per lane by commit groups and published to the warp by __syncwarp, and nothing
+// spins: cp.async.wait_group returns once the lane's own copies have landed.
+// Lane l copies neighbour block l / 4 (chunks l % 4, l % 4 + 4, ...); the link block and the
+// epilogue blocks are spread over all lanes.  With NST stages the copies of the warp's next
+// NST - 1 sites are in flight while it computes one site.
+__device__ __forceinline__ void lcp16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void lcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void lcp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// stages per warp: three while four warps' stages stay within 80 KB (so that at least two
+// blocks fit an SM), else two
+__host__ __device__ constexpr int astages(int nc, int m, int nx) {
+    return kTWarps * 3 * tstage_bytes(nc, m, nx) <= 80 * 1024 ? 3 : 2;
+}
+
+template <typename S, int NC, bool DAG, int EPI, int NTC>
+__global__ void __launch_bounds__(kTThreads) hop_mmal_async_kernel(const HopParams p) {
+    using M = LMma<S>;
+    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
+    constexpr int NVR = NV > 0 ? NV : 1;
+    constexpr int NX = EPI == EPI_PLAIN ? 0 : ((EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 2 : 1);
+    constexpr int MR = 4 * NTC;                  // RHS count
+    constexpr uint32_t N2 = NC * NC;
+    constexpr int SW = 4 * NC * MR;              // words of a site block
+    constexpr int SBY = 4 * SW;                  // its bytes
+    constexpr int LW = 8 * NC * NC;              // words of a link block
+    constexpr int STW = tstage_bytes(NC, MR, NX) / 4;
+    constexpr int NST = astages(NC, MR, NX);
+    constexpr int NCH = NC * MR / 4;             // 16-byte chunks per lane of a neighbour block
+    constexpr int LCH = 2 * NC * NC;             // chunks of the link block
+    constexpr int XCH = NC * MR;                 // chunks of an epilogue block
+    constexpr int ECH = LCH + NX * XCH;
+    constexpr int EJ = (ECH + 31) / 32;
+    constexpr int SF = DAG ? 1 : -1;
+    static_assert(NC >= 2 && NC <= 4 && MR <= 16, "staged hop: N <= 4, m <= 16");
+    static_assert(NCH * 64 == SBY, "four lanes per neighbour block");
+    extern __shared__ __align__(16) unsigned char tsm[];
+    if (skip_launch(p.done, p.gate)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3, hh = g & 1, q = g >> 1;
+    const int cls = g >> 2, cc = g & 3;
+    const int ccl = min(cc, NC - 1), ct = min(t, NC - 1);
+    const uint32_t okm = (cc < NC && t < NC) ? 0xffffffffu : 0u;
+    const bool sok = cc < NC;
+    const int oa = (hh * NC + ct) * MR + q;
+    const int ob01 = ((3 - hh) * NC + ct) * MR + q;
+    const int ob23 = ((2 + hh) * NC + ct) * MR + q;
+    const int os = (2 * cls * NC + ccl) * MR + t;
+    constexpr int osn = NC * MR;
+    const int lo = ccl * NC + ct;                // the lane's element of a link matrix
+    const uint32_t m1f = hh ? unit_pair<S>(SF, SF) : unit_pair<S>(-SF, -SF);
+    const uint32_t m2f = hh ? unit_pair<S>(SF, -SF) : unit_pair<S>(-SF, SF);
+    const uint32_t m1b = m1f ^ 0x80008000u, m2b = m2f ^ 0x80008000u;
+    const LPhase ph0 = lphase_lane<LRecon<0, SF>::C2>(cls != 0);
+    const LPhase ph1 = lphase_lane<LRecon<1, SF>::C2>(cls != 0);
+    const LPhase ph2 = lphase_lane<LRecon<2, SF>::C2>(cls != 0);
+    const LPhase ph3 = lphase_lane<LRecon<3, SF>::C2>(cls != 0);
+    const float fl = cls ? -1.f : 1.f;
+
+    const uint32_t vh = (uint32_t)p.g.vh;
+    const int parity = p.parity;
+    const unsigned char* __restrict__ in = static_cast<const unsigned char*>(p.in);
+    const unsigned char* __restrict__ lbase =
+        static_cast<const unsigned char*>(p.links) + (size_t)parity * vh * (LW * 4);
+    const unsigned char* __restrict__ xv = static_cast<const unsigned char*>(p.x);
+    const unsigned char* __restrict__ yv = static_cast<const unsigned char*>(p.r0);
+    const uint32_t* __restrict__ nbr = p.nbr + (size_t)parity * vh * 8;
+    uint32_t* __restrict__ out = static_cast<uint32_t*>(p.out);
+
+    uint32_t* stage = reinterpret_cast<uint32_t*>(tsm) + (size_t)warp * NST * STW;
+    const uint32_t stage_s = lsmem(stage);
+    const int nbl = lane >> 2;                   // the neighbour block this lane copies
+    const uint32_t nboff = (uint32_t)(lane & 3) * 16;
+    // copies of `site` (neighbour nbi of this lane's block) into stage k, as one commit group
+    auto issue = [&](int k, uint32_t site, uint32_t nbi) {
+        const uint32_t dst = stage_s + (uint32_t)k * (STW * 4);
+        const unsigned char* src = in + (size_t)nbi * SBY + nboff;
+        const uint32_t d0 = dst + (uint32_t)nbl * SBY + nboff;
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) lcp16(d0 + 64 * j, src + 64 * j);
+#pragma unroll
+        for (int j = 0; j < EJ; ++j) {
+            const int e = lane + 32 * j;
+            if (e < LCH) {
+                lcp16(dst + 8 * SBY + 16 * e, lbase + (size_t)site * (LW * 4) + 16 * e);
+            } else if (e < ECH) {
+                const int e2 = e - LCH;
+                const int which = e2 >= XCH;     // 0: x, 1: r0
+                const int off = e2 - which * XCH;
+                lcp16(dst + 8 * SBY + LW * 4 + which * SBY + 16 * off,
+                      (which ? yv : xv) + (size_t)site * SBY + 16 * off);
+            }
+        }
+    };
+
+    float2 red[NTC][NVR];
+#pragma unroll
+    for (int n = 0; n < NTC; ++n)
+#pragma unroll
+        for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
+
+    const uint32_t gw = blockIdx.x * kTWarps + warp;
+    const uint32_t nw = gridDim.x * kTWarps;
+    // prologue: the first NST - 1 sites (one commit group per site slot, empty past the end)
+    uint32_t pre = gw;
+#pragma unroll
+    for (int k = 0; k < NST - 1; ++k, pre += nw) {
+        if (pre < vh) issue(k, pre, __ldg(nbr + (size_t)pre * 8 + nbl));
+        lcp_commit();
+    }
+    // neighbour index of the next site to issue, loaded one site ahead
+    uint32_t nb_next = pre < vh ? __ldg(nbr + (size_t)pre * 8 + nbl) : 0u;
+    int k = 0;                                   // stage of the current site
+    for (uint32_t site = gw; site < vh; site += nw) {
+        const uint32_t nxt = site + (NST - 1) * nw;
+        if (nxt < vh) {   // its stage was released by the __syncwarp that ended the last site
+            issue(k == 0 ? NST - 1 : k - 1, nxt, nb_next);
+            nb_next = nxt + nw < vh ? __ldg(nbr + (size_t)(nxt + nw) * 8 + nbl) : 0u;
+        }
+        lcp_commit();
+        lcp_wait<NST - 1>();                     // this lane's copies of `site` have landed
+        __syncwarp();                            // ... and every lane's
+        const uint32_t* sb = stage + k * STW;       // neighbour blocks
+        const uint32_t* lk = sb + 8 * SW + lo;      // links
+        const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
+        k = k + 1 == NST ? 0 : k + 1;
+        float Qxy[NTC][4], Qzt[NTC][4];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
+        uint32_t A[4];
+        mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
+        mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
+                                  m1f, m1b);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qxy[n][0] *= fl;
+            Qxy[n][2] *= fl;
+        }
+        mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
+        mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u);
+        mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
+        mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
+                                  m2f, m2b);
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            Qzt[n][1] *= fl;
+            Qzt[n][3] *= fl;
+        }
+        mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
+        mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
+                                  0u, 0u);
+        const size_t ob = (size_t)site * SW + os;
+#pragma unroll
+        for (int n = 0; n < NTC; ++n) {
+            float2 ov[2];
+            ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
+            ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
+            ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
+            ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
+            if constexpr (EPI == EPI_PLAIN) {
+                const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
+                if (sok) {
+                    out[ob + 4 * n] = w0;
+                    out[ob + 4 * n + osn] = w1;
+                }
+            } else if (sok) {
+                const float a = (float)p.a;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const uint32_t xw = ep[4 * n + (e ? osn : 0)];
+                    const float2 xx = M::unpack(xw);
+                    float2 res;
+                    if (EPI == EPI_XPAY) {
+                        res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
+                    } else if (EPI == EPI_RESID) {
+                        const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                        res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
+                    } else {
+                        res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
+                    }
+                    const uint32_t rs = M::pack(res.x, res.y);
+                    out[ob + 4 * n + (e ? osn : 0)] = rs;
+                    if constexpr (NV > 0) {
+                        const float2 rr = M::unpack(rs);
+                        if (EPI == EPI_RESID) {
+                            red[n][0].x += rr.x * rr.x + rr.y * rr.y;
+                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
+                            const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                            red[n][0].x += qq.x * rr.x + qq.y * rr.y;
+                            red[n][0].y += qq.x * rr.y - qq.y * rr.x;
+                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
+                            red[n][0].x += rr.x * xx.x + rr.y * xx.y;
+                            red[n][0].y += rr.x * xx.y - rr.y * xx.x;
+                            red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();   // every lane has read this stage before it is refilled
+    }
+    lcp_wait<0>();      // no copy outlives the kernel (only empty groups remain at this point)
+    if constexpr (NV > 0) {
+        __shared__ double2 wsum[kTWarps][NV][kLMaxChunkRhs];
+        __shared__ double2 bsum[NV * kMaxRhs];
+#pragma unroll
+        for (int n = 0; n < NTC; ++n)
+#pragma unroll
+            for (int kk = 0; kk < NV; ++kk) {
+                double vx = (double)red[n][kk].x, vy = (double)red[n][kk].y;
+#pragma unroll
+                for (int off = 4; off < 32; off <<= 1) {
+                    vx += __shfl_xor_sync(0xffffffffu, vx, off);
+                    vy += __shfl_xor_sync(0xffffffffu, vy, off);
+                }
+                if (g == 0) wsum[warp][kk][4 * n + t] = make_double2(vx, vy);
+            }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NV * MR; idx += blockDim.x) {
+            const int kk = idx / MR, rhs = idx - kk * MR;
+            double2 s = make_double2(0.0, 0.0);
+            for (int w = 0; w < kTWarps; ++w) {
+                s.x += wsum[w][kk][rhs].x;
+                s.y += wsum[w][kk][rhs].y;
+            }
+            bsum[idx] = s;
+        }
+        __syncthreads();
+        publish_and_finish<NV>(bsum, MR, p.red);
+    }
+}
+
+template <typename S, int NC, int NTC, int EPI, bool DAG>
+void* async_kernel_ptr() {
+    return reinterpret_cast<void*>(hop_mmal_async_kernel<S, NC, DAG, EPI, NTC>);
+}
+
+template <typename S, int NC, int NTC>
+int launch_mmal_async(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+    void (*k)(const HopParams) = nullptr;
+    switch (epi) {
+        case EPI_PLAIN: k = dagger ? hop_mmal_async_kernel<S, NC, true, EPI_PLAIN, NTC> : hop_mmal_async_kernel<S, NC, false, EPI_PLAIN, NTC>; break;
+        case EPI_XPAY: k = dagger ? hop_mmal_async_kernel<S, NC, true, EPI_XPAY, NTC> : hop_mmal_async_kernel<S, NC, false, EPI_XPAY, NTC>; break;
+        case EPI_SCHUR_R0: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR_R0, NTC>; break;
+        case EPI_SCHUR_TS: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR_TS, NTC>; break;
+        case EPI_SCHUR: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR, NTC>; break;
+        case EPI_RESID: k = hop_mmal_async_kernel<S, NC, false, EPI_RESID, NTC>; break;
+        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
+    }
+    const int nx = epi == EPI_PLAIN ? 0 : ((epi == EPI_SCHUR_R0 || epi == EPI_RESID) ? 2 : 1);
+    const size_t smem = (size_t)kTWarps * astages(NC, 4 * NTC, nx) * tstage_bytes(NC, 4 * NTC, nx);
+    int grid = resident_grid(k, kTThreads, p.g.vh * 32, smem);
+    if (grid > kScratchBlocks) grid = kScratchBlocks;
+    k<<<grid, kTThreads, smem, st>>>(p);
+    QCUB_CHECK_LAUNCH();
+    return QCU_SUCCESS;
+}
+
 template <typename S, int NC, int NTC, int EPI, bool DAG>
 void* tma_kernel_ptr() {
     return reinterpret_cast<void*>(hop_mmal_tma_kernel<S, NC, DAG, EPI, NTC>);
@@ -807,7 +914,10 @@ int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, cudaStre
     const bool pre = p.links != nullptr && p.nbr != nullptr;
     if (pre && nchunk == 1 && p.m == 4 * NTC && lalign16(p.in) && lalign16(p.links) &&
         (!p.x || lalign16(p.x)) && (!p.r0 || lalign16(p.r0)))
-        return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
+    {
+        if (std::getenv("QCU_XP_TMA")) return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
+        return launch_mmal_async<S, NC, NTC>(p, dagger, epi, st);
+    }
     if (p.m == 4 * NTC * nchunk)
         return pre ? launch_mmal_t<S, NC, NTC, true, true>(p, dagger, epi, nchunk, st)
                    : launch_mmal_t<S, NC, NTC, true, false>(p, dagger, epi, nchunk, st);
@@ -853,6 +963,17 @@ cudaError_t mmal_tma_optin() {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
         if (e != cudaSuccess) return e;
     }
+    const void* ak[8] = {async_kernel_ptr<S, NC, NTC, EPI_PLAIN, false>(), async_kernel_ptr<S, NC, NTC, EPI_PLAIN, true>(),
+                         async_kernel_ptr<S, NC, NTC, EPI_XPAY, false>(), async_kernel_ptr<S, NC, NTC, EPI_XPAY, true>(),
+                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR_R0, false>(),
+                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR_TS, false>(),
+                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR, false>(), async_kernel_ptr<S, NC, NTC, EPI_RESID, false>()};
+    int aneed = 0;
+    for (int nx = 0; nx <= 2; ++nx) aneed = std::max(aneed, kTWarps * astages(NC, 4 * NTC, nx) * tstage_bytes(NC, 4 * NTC, nx));
+    for (const void* k : ak) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, aneed);
+        if (e != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 template <typename S, int NC>
@@ -883,7 +1004,7 @@ int hop_mmal_prepare() {
 }
 
 bool hop_mmal_supported(int nc, int m, int prec) {
-    return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc >= 2 && nc <= 4 && m >= 1 &&
+    return (prec == QCU_PRECISION_HALF || prec == QCU_PRECISION_BF16) && nc >= 2 && nc <= 8 && m >= 1 &&
            m <= kMaxRhs;
 }
 
@@ -898,6 +1019,7 @@ int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, 
     // 32-bit word offsets: every spinor word index below 2^31
     if (p.g.vh * 4 * nc * (int64_t)p.m >= ((int64_t)1 << 31) || p.g.vh * 8 * nc * nc >= ((int64_t)1 << 31))
         return set_error(QCU_ERR_UNSUPPORTED, "link-operand tensor-core hop: field beyond 2^31 complex");
+    if (nc >= 5) return hop_mmal_big_launch(p, nc, prec, dagger, epi, st);
     if (prec == QCU_PRECISION_HALF) return launch_mmal<__half>(p, nc, dagger, epi, st);
     return launch_mmal<__nv_bfloat16>(p, nc, dagger, epi, st);
 }

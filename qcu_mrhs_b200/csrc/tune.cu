@@ -6,6 +6,7 @@
 #include <tuple>
 
 #include "dslash.h"
+#include "workspace.h"
 
 namespace qcub {
 
@@ -77,38 +78,51 @@ int tuned_hop(int nc, int m, int prec) {
     return it == g_tuned.end() ? 0 : it->second;
 }
 
-// Returns the fastest kind (>= 1) or a negative status.
+// Returns the fastest kind (>= 1) or a negative status.  Each candidate is timed on the
+// hops of one Schur BiCGStab iteration as the solver launches them (tmp = D_eo p;
+// v = p - k^2 D_oe tmp with <r0, v>; tmp = D_eo s; t = s - k^2 D_oe tmp with <t, s>, <t, t>),
+// so the epilogues and fused reductions weigh as they do in a solve; kernels that read the
+// per-site tables (neighbour table, hop links) get them, as the solver's context provides.
 int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* best_us) {
     if (!prec_valid(prec)) return -set_error(QCU_ERR_INVALID, "precision %d", prec);
+    // kernel attributes the candidates need (outside any graph capture, as the tuner is)
+    if (int e = hop16_pairs_prepare()) return -e;
+    if (int e = hop_mmal_prepare()) return -e;
     const Geom g = make_geom(L);
     const size_t rb = prec_bytes(prec) * 2;   // bytes of one complex
     const size_t spin_bytes = (size_t)g.vh * 4 * nc * m * rb;
     const size_t gauge_bytes = (size_t)8 * g.vh * nc * nc * rb;
-    void *in = nullptr, *out = nullptr, *gauge = nullptr;
+    void *in = nullptr, *out = nullptr, *x = nullptr, *r0 = nullptr, *gauge = nullptr, *links = nullptr;
+    uint32_t* nbr = nullptr;
+    Scratch ws{};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = QCU_SUCCESS;
     auto cleanup = [&]() {
-        if (in) cudaFree(in);
-        if (out) cudaFree(out);
-        if (gauge) cudaFree(gauge);
+        for (void* ptr : {in, out, x, r0, gauge, links, static_cast<void*>(nbr)})
+            if (ptr) cudaFree(ptr);
+        scratch_free(&ws);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
     };
     if (cudaMalloc(&in, spin_bytes) != cudaSuccess || cudaMalloc(&out, spin_bytes) != cudaSuccess ||
+        cudaMalloc(&x, spin_bytes) != cudaSuccess || cudaMalloc(&r0, spin_bytes) != cudaSuccess ||
         cudaMalloc(&gauge, gauge_bytes) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
         cudaEventCreate(&e1) != cudaSuccess) {
         cudaGetLastError();
         cleanup();
         return -set_error(QCU_ERR_ALLOC, "autotuner: device allocation failed");
     }
+    if ((rc = scratch_alloc(&ws))) {
+        cleanup();
+        return -rc;
+    }
     fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(in), (int64_t)(spin_bytes / 4), 1u);
+    fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(x), (int64_t)(spin_bytes / 4), 3u);
+    fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(r0), (int64_t)(spin_bytes / 4), 4u);
     fill_kernel<<<512, 256, 0, st>>>(static_cast<uint32_t*>(gauge), (int64_t)(gauge_bytes / 4), 2u);
     const int saved = hop_kind();
     // PACKED16_ACC16 is not a candidate: it trades accuracy for speed, so only an explicit
-    // request selects it.  Nor is MMA16: the tuner times the plain hop, where MMA16 can be
-    // the faster one, but its Schur and residual forms (two of the four hops of a solver
-    // iteration) are slower than PACKED16_PAIRS's, and the solve with it is slower (B200,
-    // 24^3x48, m = 12, FP16: 87.3 ms against 81.6 ms)
+    // request selects it.  Nor is MMA16 (the link-operand kernel supersedes it).
     int kinds[6] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
                     QCU_HOP_MMA_LINK};
     int best = QCU_HOP_SIMT;
@@ -120,24 +134,44 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         if (kind == QCU_HOP_PACKED16_PAIRS && !hop16_pairs_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_MMA_LINK && !hop_mmal_supported(nc, m, prec)) continue;
         set_hop_kind(kind);
+        const bool tables = hop_reads_tables(nc, m, prec);
+        if (tables && !links) {
+            const size_t lb = hop_links_bytes(g, nc, prec), nb = neighbour_table_bytes(g);
+            if (cudaMalloc(&links, lb) != cudaSuccess || cudaMalloc(&nbr, nb) != cudaSuccess) {
+                cudaGetLastError();
+                rc = set_error(QCU_ERR_ALLOC, "autotuner: device allocation failed");
+                break;
+            }
+            if ((rc = build_neighbour_table(nbr, nb, g, st))) break;
+            if ((rc = build_hop_links(links, lb, gauge, nbr, g, nc, prec, 1.0, st))) break;
+        }
         HopParams p{};
-        p.in = in;
-        p.out = out;
         p.gauge = gauge;
         p.g = g;
         p.m = m;
         p.t_sign = 1.0;
-        for (int i = 0; i < 2 && rc == QCU_SUCCESS; ++i) {
-            p.parity = i & 1;
-            rc = hop_launch(p, nc, prec, false, EPI_PLAIN, st);
+        p.a = 0.01;
+        p.links = tables ? links : nullptr;
+        p.nbr = tables ? nbr : nullptr;
+        auto iteration = [&]() -> int {
+            int e;
+            p.out = out; p.in = in; p.x = nullptr; p.r0 = nullptr; p.parity = 0;
+            p.red = RedArgs{ws.partials, ws.counter, ws.result, nullptr, nullptr, FIN_NONE};
+            if ((e = hop_launch(p, nc, prec, false, EPI_PLAIN, st))) return e;
+            p.out = in; p.in = out; p.x = x; p.r0 = r0; p.parity = 1;
+            if ((e = hop_launch(p, nc, prec, false, EPI_SCHUR_R0, st))) return e;
+            p.out = out; p.in = in; p.x = nullptr; p.r0 = nullptr; p.parity = 0;
+            if ((e = hop_launch(p, nc, prec, false, EPI_PLAIN, st))) return e;
+            p.out = in; p.in = out; p.x = x; p.r0 = nullptr; p.parity = 1;
+            return hop_launch(p, nc, prec, false, EPI_SCHUR_TS, st);
+        };
+        if (iteration()) {   // warm-up; a kernel without one of the solver's forms is no candidate
+            clear_error();
+            continue;
         }
-        if (rc) break;
-        const int reps = 5;
+        const int reps = 3;
         cudaEventRecord(e0, st);
-        for (int i = 0; i < reps && rc == QCU_SUCCESS; ++i) {
-            p.parity = i & 1;
-            rc = hop_launch(p, nc, prec, false, EPI_PLAIN, st);
-        }
+        for (int i = 0; i < reps && rc == QCU_SUCCESS; ++i) rc = iteration();
         cudaEventRecord(e1, st);
         if (rc) break;
         if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -153,6 +187,7 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         }
     }
     set_hop_kind(saved);
+    cudaStreamSynchronize(st);
     cleanup();
     if (rc) return -rc;
     {
@@ -187,4 +222,10 @@ extern "C" int qcuTuneHop(const int L[4], int n_color, int m_rhs, int precision,
 
 extern "C" int qcuGetTunedHop(int n_color, int m_rhs, int precision) {
     return tuned_hop(n_color, m_rhs, precision);
+}
+
+extern "C" int qcuGetAutoHop(int n_color, int m_rhs, int precision) {
+    if (n_color < 2 || n_color > kMaxColor || m_rhs < 1 || m_rhs > kMaxRhs || !prec_valid(precision))
+        return -set_error(QCU_ERR_INVALID, "shape n_color=%d m_rhs=%d precision=%d", n_color, m_rhs, precision);
+    return auto_hop_kind(n_color, m_rhs, precision);
 }

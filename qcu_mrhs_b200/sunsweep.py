@@ -1,19 +1,24 @@
 """SU(N) generality sweep of the multi-RHS hop: every kernel that covers a shape, timed
 through the C ABI (qcuDslashMrhs) with CUDA events.
 
-  python -m qcu_mrhs_b200.sunsweep [--L 16 16 16 16] [--nc 3 4 6 8] [--m 8 16 32]
-                                   [--prec f64 f32 bf16] [--reps 20]
+  python -m qcu_mrhs_b200.sunsweep [--L 16 16 16 16] [--nc 2 3 4 5 6 7 8] [--m 8 16 32]
+                                   [--prec f64 f32 f16 bf16] [--reps 20] [--out FILE]
 
 Prints one JSON line per (N, m, precision, kernel) with the launch time, algorithmic
-GB/s and GFLOP/s (hopbench's definitions), and a closing line with the fastest kernel
-per (N, m, precision).  Kernels: simt (one thread per site and RHS), simt_cs (colour
-split), tcgen05 (tensor cores, FP16/BF16, N <= 4), packed16 (packed 16-bit arithmetic,
-FP16/BF16, N <= 4).  Inputs are random device tensors; values do not affect timing.
+GB/s and GFLOP/s (hopbench's definitions) and the fraction of the HBM copy bandwidth
+(MEASURED_PEAKS.json at the repository root, else 6650 GB/s), and a closing line with the
+fastest kernel per (N, m, precision) and, per (N, m), the speed-up of the fastest 16-bit
+kernel over the fastest FP32 one.  --out also writes all of it as one JSON document.
+Kernels: simt (one thread per site and RHS), simt_cs (colour split), tcgen05 (tensor
+cores, FP16/BF16, N <= 4), packed16 (packed 16-bit arithmetic, FP16/BF16, N <= 4),
+mma_link (warp MMA with the links as the A operand, FP16/BF16, 2 <= N <= 8).  Inputs are
+random device tensors; values do not affect timing.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import os
 
 from .hopbench import KERNELS, run
 
@@ -28,19 +33,33 @@ def applicable(kernel, nc, m, prec):
         return low and 2 <= nc <= 4 and 4 * m <= 128
     if kernel == "packed16":
         return low and 2 <= nc <= 4 and m >= 2
+    if kernel == "mma_link":
+        return low and 2 <= nc <= 8
     return False
+
+
+def hbm_peak():
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--L", type=int, nargs=4, default=[16, 16, 16, 16])
-    ap.add_argument("--nc", type=int, nargs="+", default=[3, 4, 6, 8])
+    ap.add_argument("--nc", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8])
     ap.add_argument("--m", type=int, nargs="+", default=[8, 16, 32])
-    ap.add_argument("--prec", nargs="+", default=["f64", "f32", "bf16"])
-    ap.add_argument("--kernels", nargs="+", default=["simt", "simt_cs", "tcgen05", "packed16"])
+    ap.add_argument("--prec", nargs="+", default=["f64", "f32", "f16", "bf16"])
+    ap.add_argument("--kernels", nargs="+", default=["simt", "simt_cs", "tcgen05", "packed16", "mma_link"])
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--out", default=None, help="also write every line as one JSON document")
     args = ap.parse_args()
+    peak, peak_kind = hbm_peak()
     best = {}
+    rows = []
     for nc in args.nc:
         for m in args.m:
             for prec in args.prec:
@@ -48,12 +67,27 @@ def main():
                     if not applicable(kname, nc, m, prec):
                         continue
                     r = run(tuple(args.L), nc, m, prec, args.reps, 3, kernel=KERNELS.index(kname))
+                    r["hbm_frac"] = r["GBps"] / peak
+                    rows.append(r)
                     print(json.dumps(r), flush=True)
                     key = f"N{nc}_m{m}_{prec}"
                     if key not in best or r["launch_us"] < best[key]["launch_us"]:
                         best[key] = {"kernel": kname, "launch_us": r["launch_us"], "GBps": r["GBps"],
-                                     "GFLOPs": r["GFLOPs"]}
-    print(json.dumps({"fastest": best}), flush=True)
+                                     "GFLOPs": r["GFLOPs"], "hbm_frac": r["hbm_frac"]}
+    # per (N, m): fastest 16-bit kernel against the fastest FP32 one (time ratio)
+    low_vs_f32 = {}
+    for nc in args.nc:
+        for m in args.m:
+            f32 = best.get(f"N{nc}_m{m}_f32")
+            for lp in ("f16", "bf16"):
+                b = best.get(f"N{nc}_m{m}_{lp}")
+                if f32 and b:
+                    low_vs_f32[f"N{nc}_m{m}_{lp}"] = f32["launch_us"] / b["launch_us"]
+    summary = {"fastest": best, "speedup_vs_f32": low_vs_f32, "hbm_peak_gbs": peak, "hbm_peak_kind": peak_kind}
+    print(json.dumps(summary), flush=True)
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump({"L": args.L, "reps": args.reps, "rows": rows, **summary}, f, indent=1)
 
 
 if __name__ == "__main__":

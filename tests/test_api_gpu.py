@@ -193,6 +193,54 @@ def _invert(L, nc, m, kappa, tol, seed, opts=None, max_iter=2000, kind="haar", t
     return gauge, b, x, st, q.solve_stats()
 
 
+def test_repeated_solves_reuse_the_iteration_graph(oracle_lib):
+    """Several qcuInvert calls on one context.  Each solve captures its block of iterations
+    again and updates the executable graph the context keeps in place (cudaGraphExecUpdate),
+    or instantiates anew when the update is refused.  The sequence covers both: FP64 with new
+    sources (same topology: updated in place), FP64 with another check_interval and mixed
+    FP16 (other topologies), mixed FP16 with the sloppy hop kernel forced to another kind
+    (same topology, other kernel nodes), and FP64 again.  Every solution meets M x = b to the
+    tolerance on the full system (oracle), and the iteration counts are plausible."""
+    L, nc, m, kappa, tol = (8, 4, 4, 8), 3, 8, 0.11, 1e-10
+    gauge, dg = _setup(L, nc, m, kappa, 41, kind="smooth")
+    vh = F.half_volume(L)
+    steps = [
+        dict(solver=q.SOLVER_FUSED, check_interval=8, seed=42, kernel=q.HOP_AUTO),
+        dict(solver=q.SOLVER_FUSED, check_interval=8, seed=43, kernel=q.HOP_AUTO),
+        dict(solver=q.SOLVER_FUSED, check_interval=4, seed=44, kernel=q.HOP_AUTO),
+        dict(solver=q.SOLVER_MIXED, check_interval=8, seed=45, kernel=q.HOP_AUTO),
+        dict(solver=q.SOLVER_MIXED, check_interval=8, seed=46, kernel=q.HOP_PACKED16_PAIRS),
+        dict(solver=q.SOLVER_MIXED, check_interval=8, seed=47, kernel=q.HOP_MMA_LINK),
+        dict(solver=q.SOLVER_FUSED, check_interval=8, seed=48, kernel=q.HOP_AUTO),
+    ]
+    try:
+        for i, stp in enumerate(steps):
+            o = q.default_options()
+            o.solver = stp["solver"]
+            o.sloppy_precision = q.HALF
+            o.check_interval = stp["check_interval"]
+            o.stop_true_residual = 1
+            o.t_boundary = -1.0
+            q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+            q.check(q.lib().qcuSetHopKernel(stp["kernel"]))
+            b = F.gaussian_fermions(L, nc, m, stp["seed"])
+            ins = [to_dev(b[j]) for j in range(m)]
+            outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+            for j in range(m):
+                q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+            q.lib().qcuInvert(2000, tol)
+            assert q.status() == q.SUCCESS, f"solve {i}: {q.last_error()}"
+            stats = q.solve_stats()
+            assert 5 <= stats.iterations <= 200, f"solve {i}: {stats.iterations} iterations"
+            x = np.stack([from_dev(v) for v in outs])
+            res = oracle_lib.mat(x, gauge, L, kappa, t_sign=-1.0) - b
+            rel = np.linalg.norm(res.reshape(m, -1), axis=1) / np.linalg.norm(b.reshape(m, -1), axis=1)
+            assert np.all(rel <= 2 * tol), f"solve {i}: {rel.max()}"
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
 def test_invert_matches_oracle_reference_rule(oracle_lib):
     """Config 1: 8^4, SU(3) Haar, m = 4, kappa = 0.10, antiperiodic t, tol 1e-10."""
     L, nc, m, kappa, tol = (8, 8, 8, 8), 3, 4, 0.10, 1e-10
