@@ -65,7 +65,9 @@ typedef struct {
     double reliable_delta;   /* MIXED: reliable update when ||r|| < delta * max ||r|| (0.1) */
     double t_boundary;       /* +1 periodic in t (reference), -1 antiperiodic in t */
     int check_interval;      /* iterations per captured graph between host checks (8) */
-    int freeze_converged;    /* 1: converged right-hand sides stop updating */
+    int freeze_converged;    /* 1: converged right-hand sides stop updating (the MIXED solver
+                                always stops an RHS whose FP64 residual converged, and its
+                                tensor-core sloppy hops skip groups of 4 stopped RHS) */
     int max_restarts;        /* MIXED: cap on reliable updates (0 = unlimited) */
     double reliable_quorum;  /* MIXED: a reliable update waits until this fraction of the
                                 unconverged RHS met the delta rule or claim convergence
@@ -160,6 +162,7 @@ int qcuSetPreconditioner(void *handle);
                                      a later batch reuses them for systems of the same lattice,
                                      n_color and m_rhs (qcuBatchRelease frees them) */
 
+/* opts = NULL: the defaults of qcuGetDefaultSolverOptions with freeze_converged = 1 */
 int qcuInvertBatch(QcuBatchSystem *systems, int n_systems, const QcuSolverOptions *opts, int flags);
 /* free the contexts kept by QCU_BATCH_KEEP_CONTEXTS */
 int qcuBatchRelease(void);
@@ -189,6 +192,12 @@ int qcuDslashMrhsXpay(void *out, const void *in, const void *gauge, const void *
  * reference's qcu::Dslash::apply on the Qcu object's gauge copies
  * (src/qcu_interface.cu:109-172 without the gather/scatter). */
 int qcuDslashMrhsContext(void *out, const void *in, int parity, int dagger, int precision, void *stream);
+/* The same with per-RHS activity flags `active` (device int[m_rhs]): the FP16/BF16
+ * tensor-core hop (QCU_HOP_MMA_LINK) skips every group of 4 RHS (0-3, 4-7, ...) whose flags
+ * are all 0 and leaves their outputs as they were; other kernels compute every RHS.  The
+ * mixed solver's sloppy hops run this way with the flags of its converged RHS. */
+int qcuDslashMrhsContextActive(void *out, const void *in, int parity, int dagger, int precision,
+                               const int *active, void *stream);
 
 /* Schur operator out_o = in_o - kappa^2 D_oe D_eo in_o; tmp is one half-lattice vector.
  * Replaces fused_x_sub_Doe_Deo_x -- reference src/solver/bicgstab_solve.cu:27-70. */

@@ -116,6 +116,7 @@ _SIGNATURES = {
     "qcuDslashMrhs": (_i, [_vp, _vp, _vp, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuDslashMrhsXpay": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuDslashMrhsContext": (_i, [_vp, _vp, _i, _i, _i, _vp]),
+    "qcuDslashMrhsContextActive": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp]),
     "qcuSchurMrhs": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _d, _i, _vp]),
     "qcuGatherMrhs": (_i, [_vp, _i, ctypes.POINTER(_vp), _i, _i64, _i, _i, _vp]),
     "qcuScatterMrhs": (_i, [ctypes.POINTER(_vp), _i, _vp, _i, _i64, _i, _i, _vp]),

@@ -525,8 +525,9 @@ int qcuDslashMrhsXpay(void* out, const void* in, const void* gauge, const void* 
                       EPI_XPAY);
 }
 
-int qcuDslashMrhsContext(void* out, const void* in, int parity, int dagger, int precision, void* stream) {
-    QCUB_API_BEGIN
+// the context's hop (caller holds the API lock)
+static int context_hop(void* out, const void* in, int parity, int dagger, int precision, const int* active,
+                       void* stream) {
     int rc = require_ctx();
     if (rc) return rc;
     Context& c = *g_ctx;
@@ -554,7 +555,20 @@ int qcuDslashMrhsContext(void* out, const void* in, int parity, int dagger, int 
     p.m = c.m;
     p.parity = parity;
     p.t_sign = c.opts.t_boundary;
+    p.active = active;
     return hop_launch(p, c.nc, precision, dagger != 0, EPI_PLAIN, st);
+}
+
+int qcuDslashMrhsContext(void* out, const void* in, int parity, int dagger, int precision, void* stream) {
+    QCUB_API_BEGIN
+    return context_hop(out, in, parity, dagger, precision, nullptr, stream);
+}
+
+int qcuDslashMrhsContextActive(void* out, const void* in, int parity, int dagger, int precision,
+                               const int* active, void* stream) {
+    QCUB_API_BEGIN
+    if (!active) return set_error(QCU_ERR_INVALID, "null activity flags");
+    return context_hop(out, in, parity, dagger, precision, active, stream);
 }
 
 int qcuSchurMrhs(void* out, const void* in, void* tmp, const void* gauge, double kappa, const int L[4],

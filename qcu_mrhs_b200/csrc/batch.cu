@@ -17,7 +17,8 @@
 //   host loop (QCU_BATCH_HOST_LOOP): each branch holds `check_interval` iterations; the host
 //     relaunches the graph and reads every system's `done` flag between launches
 //     (converged systems' kernels return at once).
-// Converged right-hand sides inside a running system are frozen with freeze_converged.
+// Converged right-hand sides inside a running system are frozen with freeze_converged (on
+// when no options are given); the mixed solver's sloppy hops skip their groups of 4 RHS.
 // Before capture, the hop kernel of every distinct (n_color, m_rhs, precision) is picked
 // by the autotuner (tune.cu) unless one is already recorded.
 #include <chrono>
@@ -224,6 +225,7 @@ int invert_batch(QcuBatchSystem* sys, int n, const QcuSolverOptions* opts_in, in
         o = *opts_in;
     } else {
         qcuGetDefaultSolverOptions(&o);
+        o.freeze_converged = 1;   // batch default: converged RHS stop (and drop out of the hops)
     }
     if (o.solver < QCU_SOLVER_REFERENCE || o.solver > QCU_SOLVER_MIXED)
         return set_error(QCU_ERR_INVALID, "solver %d", o.solver);

@@ -51,6 +51,9 @@ struct HopParams {
     // hop-link array in the storage precision built for this t_sign, and neighbour table
     const void* links;
     const uint32_t* nbr;
+    // optional per-RHS flags (device int[m]): the tensor-core hop skips every group of 4 RHS
+    // whose flags are all 0 (its outputs are then left as they were); null = all active
+    const int* active;
 };
 
 __device__ __forceinline__ bool skip_launch(const int* done, const int* gate) {

@@ -1,8 +1,5 @@
 // dslash_mmal.cu -- the link-operand tensor-core hop for N <= 4 (fragment scheme in
 // dslash_mmal.cuh) and the public entry points of the link-operand hop.
-#include <algorithm>
-#include <cstdlib>
-
 #include "dslash_mmal.cuh"
 
 namespace qcub {
@@ -17,13 +14,13 @@ template <typename S, int MU, int SF, int NTC, bool EXACT>
 __device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __restrict__ pf,
                                          const uint32_t* __restrict__ qf, const uint32_t* __restrict__ pb,
                                          const uint32_t* __restrict__ qb, const uint32_t (&A)[4], uint32_t lmf,
-                                         uint32_t lmb, int rb0, int q, int m) {
+                                         uint32_t lmb, int rb0, int q, int m, uint32_t gmask) {
     using M = LMma<S>;
     constexpr int SB = -SF;
     uint32_t w[NTC][4];
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
+        if (!((gmask >> n) & 1u)) continue;   // warp-uniform: absent or inactive group
         int d = 4 * n;
         if (!EXACT) d += min(0, m - 1 - (rb0 + 4 * n + q));   // last partial group: clamp the RHS
         w[n][0] = __ldg(pf + d);
@@ -33,7 +30,7 @@ __device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __r
     }
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!EXACT && rb0 + 4 * n >= m) break;
+        if (!((gmask >> n) & 1u)) continue;
         const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
         const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
         M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
@@ -105,6 +102,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
     const uint32_t site_stride = (uint32_t)(nw / nchunk);
     const uint32_t site0 = gw < (int64_t)site_stride * nchunk ? (uint32_t)(gw / nchunk) : vh;
     const int rb0 = chunk * NTC * 4;
+    const uint32_t gmask = active_groups<NTC>(p.active, rb0, m);
     const uint32_t* __restrict__ inA = in + rb0 + (hh * NC + ct) * m;
     const uint32_t* __restrict__ inB01 = in + rb0 + ((3 - hh) * NC + ct) * m;
     const uint32_t* __restrict__ inB23 = in + rb0 + ((2 + hh) * NC + ct) * m;
@@ -162,7 +160,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
 #pragma unroll
             for (int n = 0; n < NTC; ++n) {
                 xw[n][0] = xw[n][1] = yw[n][0] = yw[n][1] = 0u;
-                if (!EXACT && rb0 + 4 * n >= m) break;
+                if (!((gmask >> n) & 1u)) continue;
                 if (sok && (EXACT || rb0 + 4 * n + t < m)) {
                     const size_t o = sbase + os + 4 * n;
                     xw[n][0] = __ldg(xv + o);
@@ -185,7 +183,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         // x - y (the y projector's spin-3 phase is minus its diff-row phase)
         mmal_a(A, wf[1], wb[1], okm, ph1.sel, ph1.mf, ph1.mb);
         mmal_dir<S, 1, SF, NTC, EXACT>(Qxy, inA + (size_t)nb2 * SW, inB01 + (size_t)nb2 * SW, inA + (size_t)nb3 * SW,
-                                       inB01 + (size_t)nb3 * SW, A, m1f, m1b, rb0, q, m);
+                                       inB01 + (size_t)nb3 * SW, A, m1f, m1b, rb0, q, m, gmask);
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
             Qxy[n][0] *= fl;
@@ -193,12 +191,12 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         }
         mmal_a(A, wf[0], wb[0], okm, ph0.sel, ph0.mf, ph0.mb);
         mmal_dir<S, 0, SF, NTC, EXACT>(Qxy, inA + (size_t)nb0 * SW, inB01 + (size_t)nb0 * SW, inA + (size_t)nb1 * SW,
-                                       inB01 + (size_t)nb1 * SW, A, 0u, 0u, rb0, q, m);
+                                       inB01 + (size_t)nb1 * SW, A, 0u, 0u, rb0, q, m, gmask);
         // z, then spin 3 (diff column h1, registers 1 and 3) negated, then t (boundary sign
         // folded into the links)
         mmal_a(A, wf[2], wb[2], okm, ph2.sel, ph2.mf, ph2.mb);
         mmal_dir<S, 2, SF, NTC, EXACT>(Qzt, inA + (size_t)nb4 * SW, inB23 + (size_t)nb4 * SW, inA + (size_t)nb5 * SW,
-                                       inB23 + (size_t)nb5 * SW, A, m2f, m2b, rb0, q, m);
+                                       inB23 + (size_t)nb5 * SW, A, m2f, m2b, rb0, q, m, gmask);
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
             Qzt[n][1] *= fl;
@@ -206,11 +204,11 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         }
         mmal_a(A, wf[3], wb[3], okm, ph3.sel, ph3.mf, ph3.mb);
         mmal_dir<S, 3, SF, NTC, EXACT>(Qzt, inA + (size_t)nb6 * SW, inB23 + (size_t)nb6 * SW, inA + (size_t)nb7 * SW,
-                                       inB23 + (size_t)nb7 * SW, A, 0u, 0u, rb0, q, m);
+                                       inB23 + (size_t)nb7 * SW, A, 0u, 0u, rb0, q, m, gmask);
 
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
-            if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
+            if (!((gmask >> n) & 1u)) continue;   // warp-uniform
             const bool rok = sok && (EXACT || rb0 + 4 * n + t < m);
             const size_t o = sbase + os + 4 * n;
             // the lane's two spins (2 cls, 2 cls + 1) of (colour g % 4, RHS t): sum lanes take
@@ -259,6 +257,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
             }
         }
     }
+
     if constexpr (NV > 0) {
         // lanes (g, t) hold RHS rb0 + 4n + t: sum over g (fixed butterfly), then over the
         // block's warps of the same chunk in order, then the common grid stage
@@ -340,12 +339,13 @@ __host__ __device__ constexpr int tstage_bytes(int nc, int m, int nx) { return (
 template <typename S, int MU, int SF, int NTC>
 __device__ __forceinline__ void mmal_dir_s(float (&Q)[NTC][4], const uint32_t* pf, const uint32_t* qf,
                                            const uint32_t* pb, const uint32_t* qb, const uint32_t (&A)[4],
-                                           uint32_t lmf, uint32_t lmb) {
+                                           uint32_t lmf, uint32_t lmb, uint32_t gmask) {
     using M = LMma<S>;
     constexpr int SB = -SF;
     uint32_t w[NTC][4];
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
+        if (!((gmask >> n) & 1u)) continue;   // warp-uniform: inactive group
         w[n][0] = pf[4 * n];
         w[n][1] = qf[4 * n];
         w[n][2] = pb[4 * n];
@@ -353,6 +353,7 @@ __device__ __forceinline__ void mmal_dir_s(float (&Q)[NTC][4], const uint32_t* p
     }
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
+        if (!((gmask >> n) & 1u)) continue;
         const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
         const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
         M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
@@ -396,6 +397,7 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
     const LPhase ph2 = lphase_lane<LRecon<2, SF>::C2>(cls != 0);
     const LPhase ph3 = lphase_lane<LRecon<3, SF>::C2>(cls != 0);
     const float fl = cls ? -1.f : 1.f;
+    const uint32_t gmask = active_groups<NTC>(p.active, 0, MR);
 
     const uint32_t vh = (uint32_t)p.g.vh;
     const int parity = p.parity;
@@ -449,118 +451,131 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
 #pragma unroll
         for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
 
-    uint32_t site = gw;
-    uint32_t inflight = 0;   // bit k: stage k has copies in flight
-    uint32_t use = 0;        // uses of each stage so far (bit k = parity of stage k's next wait)
-    if (site < vh) {
-        issue(0, site, lane < 8 ? __ldg(nbr + (size_t)site * 8 + lane) : 0u);
-        inflight |= 1u;
-    }
-    // neighbour index of the next site, loaded one site ahead
-    uint32_t nb_next = (site + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(site + nw) * 8 + lane) : 0u;
-    bool ok = true;
-    for (int it = 0; site < vh; ++it, site += nw) {
-        const int k = it & 1;
-        const uint32_t nxt = site + nw;
-        if (nxt < vh) {   // the other stage was released by the previous site's __syncwarp
-            issue(k ^ 1, nxt, nb_next);
-            inflight |= 2u >> k;
-            nb_next = (nxt + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(nxt + nw) * 8 + lane) : 0u;
+    // the warp's sites; MASKED: some group of 4 RHS is inactive.  Both forms are compiled so
+    // that the all-active case keeps straight-line code (no per-group branches between the
+    // loads of successive groups).
+    auto sites = [&](auto masked) {
+        constexpr bool MASKED = decltype(masked)::value;
+        const uint32_t gm = MASKED ? gmask : (1u << NTC) - 1u;
+        uint32_t site = gw;
+        uint32_t inflight = 0;   // bit k: stage k has copies in flight
+        uint32_t use = 0;        // uses of each stage so far (bit k = parity of stage k's next wait)
+        if (site < vh) {
+            issue(0, site, lane < 8 ? __ldg(nbr + (size_t)site * 8 + lane) : 0u);
+            inflight |= 1u;
         }
-        if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) {
-            ok = false;
-            break;
-        }
-        use ^= 1u << k;
-        inflight &= ~(1u << k);
-        const uint32_t* sb = stage + k * STW;       // neighbour blocks
-        const uint32_t* lk = sb + 8 * SW + lo;      // links
-        const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
-        float Qxy[NTC][4], Qzt[NTC][4];
+        // neighbour index of the next site, loaded one site ahead
+        uint32_t nb_next = (site + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(site + nw) * 8 + lane) : 0u;
+        bool ok = true;
+        for (int it = 0; site < vh; ++it, site += nw) {
+            const int k = it & 1;
+            const uint32_t nxt = site + nw;
+            if (nxt < vh) {   // the other stage was released by the previous site's __syncwarp
+                issue(k ^ 1, nxt, nb_next);
+                inflight |= 2u >> k;
+                nb_next = (nxt + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(nxt + nw) * 8 + lane) : 0u;
+            }
+            if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) {
+                ok = false;
+                break;
+            }
+            use ^= 1u << k;
+            inflight &= ~(1u << k);
+            const uint32_t* sb = stage + k * STW;       // neighbour blocks
+            const uint32_t* lk = sb + 8 * SW + lo;      // links
+            const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
+            float Qxy[NTC][4], Qzt[NTC][4];
 #pragma unroll
-        for (int n = 0; n < NTC; ++n)
+            for (int n = 0; n < NTC; ++n)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
-        uint32_t A[4];
-        mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
-        mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
-                                  m1f, m1b);
+                for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
+            uint32_t A[4];
+            mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
+            mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
+                                      m1f, m1b, gm);
 #pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            Qxy[n][0] *= fl;
-            Qxy[n][2] *= fl;
-        }
-        mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
-        mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u);
-        mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
-        mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
-                                  m2f, m2b);
+            for (int n = 0; n < NTC; ++n) {
+                Qxy[n][0] *= fl;
+                Qxy[n][2] *= fl;
+            }
+            mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
+            mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u, gm);
+            mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
+            mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
+                                      m2f, m2b, gm);
 #pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            Qzt[n][1] *= fl;
-            Qzt[n][3] *= fl;
-        }
-        mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
-        mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
-                                  0u, 0u);
-        const size_t ob = (size_t)site * SW + os;
+            for (int n = 0; n < NTC; ++n) {
+                Qzt[n][1] *= fl;
+                Qzt[n][3] *= fl;
+            }
+            mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
+            mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
+                                      0u, 0u, gm);
+            const size_t ob = (size_t)site * SW + os;
 #pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            float2 ov[2];
-            ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
-            ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
-            ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
-            ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
-            if constexpr (EPI == EPI_PLAIN) {
-                const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
-                if (sok) {
-                    out[ob + 4 * n] = w0;
-                    out[ob + 4 * n + osn] = w1;
-                }
-            } else if (sok) {
-                const float a = (float)p.a;
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const uint32_t xw = ep[4 * n + (e ? osn : 0)];
-                    const float2 xx = M::unpack(xw);
-                    float2 res;
-                    if (EPI == EPI_XPAY) {
-                        res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
-                    } else if (EPI == EPI_RESID) {
-                        const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
-                        res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
-                    } else {
-                        res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
+            for (int n = 0; n < NTC; ++n) {
+                if (!((gm >> n) & 1u)) continue;
+                float2 ov[2];
+                ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
+                ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
+                ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
+                ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
+                if constexpr (EPI == EPI_PLAIN) {
+                    const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
+                    if (sok) {
+                        out[ob + 4 * n] = w0;
+                        out[ob + 4 * n + osn] = w1;
                     }
-                    const uint32_t rs = M::pack(res.x, res.y);
-                    out[ob + 4 * n + (e ? osn : 0)] = rs;
-                    if constexpr (NV > 0) {
-                        const float2 rr = M::unpack(rs);
-                        if (EPI == EPI_RESID) {
-                            red[n][0].x += rr.x * rr.x + rr.y * rr.y;
-                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
-                            const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
-                            red[n][0].x += qq.x * rr.x + qq.y * rr.y;
-                            red[n][0].y += qq.x * rr.y - qq.y * rr.x;
-                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
-                            red[n][0].x += rr.x * xx.x + rr.y * xx.y;
-                            red[n][0].y += rr.x * xx.y - rr.y * xx.x;
-                            red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                } else if (sok) {
+                    const float a = (float)p.a;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const uint32_t xw = ep[4 * n + (e ? osn : 0)];
+                        const float2 xx = M::unpack(xw);
+                        float2 res;
+                        if (EPI == EPI_XPAY) {
+                            res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
+                        } else if (EPI == EPI_RESID) {
+                            const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                            res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
+                        } else {
+                            res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
+                        }
+                        const uint32_t rs = M::pack(res.x, res.y);
+                        out[ob + 4 * n + (e ? osn : 0)] = rs;
+                        if constexpr (NV > 0) {
+                            const float2 rr = M::unpack(rs);
+                            if (EPI == EPI_RESID) {
+                                red[n][0].x += rr.x * rr.x + rr.y * rr.y;
+                            } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
+                                const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                                red[n][0].x += qq.x * rr.x + qq.y * rr.y;
+                                red[n][0].y += qq.x * rr.y - qq.y * rr.x;
+                            } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
+                                red[n][0].x += rr.x * xx.x + rr.y * xx.y;
+                                red[n][0].y += rr.x * xx.y - rr.y * xx.x;
+                                red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                            }
                         }
                     }
                 }
             }
+            __syncwarp();   // every lane has read stage k before it is refilled
         }
-        __syncwarp();   // every lane has read stage k before it is refilled
-    }
-    if (!ok) {
-        // a wait gave up: record it and let the copies still in flight land (bounded)
-        if (lane == 0) atomicExch(err, 1);
-        for (int k = 0; k < kTStages; ++k)
-            if ((inflight >> k) & 1u) {
-                if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) break;
-            }
-    }
+        if (!ok) {
+            // a wait gave up: record it and let the copies still in flight land (bounded)
+            if (lane == 0) atomicExch(err, 1);
+            for (int k = 0; k < kTStages; ++k)
+                if ((inflight >> k) & 1u) {
+                    if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) break;
+                }
+        }
+    };
+    if (gmask == (1u << NTC) - 1u)
+        sites(std::false_type{});
+    else
+        sites(std::true_type{});
+
     if constexpr (NV > 0) {
         __shared__ double2 wsum[kTWarps][NV][kLMaxChunkRhs];
         __shared__ double2 bsum[NV * kMaxRhs];
@@ -589,274 +604,6 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
         __syncthreads();
         publish_and_finish<NV>(bsum, MR, p.red);
     }
-}
-
-// ---------------------------------------------------------------------------------
-// Asynchronous-copy variant of the staged kernel: the same stage layout, filled by the
-// lanes' own 16-byte asynchronous copies (cp.async.cg: global through L2 into shared memory)
-// instead of bulk copies.  Each lane gives its own addresses at no extra cost (a bulk copy
-// takes warp-uniform operands, so per-lane ones are issued one lane at a time), completion
-// is tracked per lane by commit groups and published to the warp by __syncwarp, and nothing
-// spins: cp.async.wait_group returns once the lane's own copies have landed.
-// Lane l copies neighbour block l / 4 (chunks l % 4, l % 4 + 4, ...); the link block and the
-// epilogue blocks are spread over all lanes.  With NST stages the copies of the warp's next
-// NST - 1 sites are in flight while it computes one site.
-__device__ __forceinline__ void lcp16(uint32_t dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void lcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void lcp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// stages per warp: three while four warps' stages stay within 80 KB (so that at least two
-// blocks fit an SM), else two
-__host__ __device__ constexpr int astages(int nc, int m, int nx) {
-    return kTWarps * 3 * tstage_bytes(nc, m, nx) <= 80 * 1024 ? 3 : 2;
-}
-
-template <typename S, int NC, bool DAG, int EPI, int NTC>
-__global__ void __launch_bounds__(kTThreads) hop_mmal_async_kernel(const HopParams p) {
-    using M = LMma<S>;
-    constexpr int NV = (EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 1 : (EPI == EPI_SCHUR_TS ? 2 : 0);
-    constexpr int NVR = NV > 0 ? NV : 1;
-    constexpr int NX = EPI == EPI_PLAIN ? 0 : ((EPI == EPI_SCHUR_R0 || EPI == EPI_RESID) ? 2 : 1);
-    constexpr int MR = 4 * NTC;                  // RHS count
-    constexpr uint32_t N2 = NC * NC;
-    constexpr int SW = 4 * NC * MR;              // words of a site block
-    constexpr int SBY = 4 * SW;                  // its bytes
-    constexpr int LW = 8 * NC * NC;              // words of a link block
-    constexpr int STW = tstage_bytes(NC, MR, NX) / 4;
-    constexpr int NST = astages(NC, MR, NX);
-    constexpr int NCH = NC * MR / 4;             // 16-byte chunks per lane of a neighbour block
-    constexpr int LCH = 2 * NC * NC;             // chunks of the link block
-    constexpr int XCH = NC * MR;                 // chunks of an epilogue block
-    constexpr int ECH = LCH + NX * XCH;
-    constexpr int EJ = (ECH + 31) / 32;
-    constexpr int SF = DAG ? 1 : -1;
-    static_assert(NC >= 2 && NC <= 4 && MR <= 16, "staged hop: N <= 4, m <= 16");
-    static_assert(NCH * 64 == SBY, "four lanes per neighbour block");
-    extern __shared__ __align__(16) unsigned char tsm[];
-    if (skip_launch(p.done, p.gate)) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, t = lane & 3, hh = g & 1, q = g >> 1;
-    const int cls = g >> 2, cc = g & 3;
-    const int ccl = min(cc, NC - 1), ct = min(t, NC - 1);
-    const uint32_t okm = (cc < NC && t < NC) ? 0xffffffffu : 0u;
-    const bool sok = cc < NC;
-    const int oa = (hh * NC + ct) * MR + q;
-    const int ob01 = ((3 - hh) * NC + ct) * MR + q;
-    const int ob23 = ((2 + hh) * NC + ct) * MR + q;
-    const int os = (2 * cls * NC + ccl) * MR + t;
-    constexpr int osn = NC * MR;
-    const int lo = ccl * NC + ct;                // the lane's element of a link matrix
-    const uint32_t m1f = hh ? unit_pair<S>(SF, SF) : unit_pair<S>(-SF, -SF);
-    const uint32_t m2f = hh ? unit_pair<S>(SF, -SF) : unit_pair<S>(-SF, SF);
-    const uint32_t m1b = m1f ^ 0x80008000u, m2b = m2f ^ 0x80008000u;
-    const LPhase ph0 = lphase_lane<LRecon<0, SF>::C2>(cls != 0);
-    const LPhase ph1 = lphase_lane<LRecon<1, SF>::C2>(cls != 0);
-    const LPhase ph2 = lphase_lane<LRecon<2, SF>::C2>(cls != 0);
-    const LPhase ph3 = lphase_lane<LRecon<3, SF>::C2>(cls != 0);
-    const float fl = cls ? -1.f : 1.f;
-
-    const uint32_t vh = (uint32_t)p.g.vh;
-    const int parity = p.parity;
-    const unsigned char* __restrict__ in = static_cast<const unsigned char*>(p.in);
-    const unsigned char* __restrict__ lbase =
-        static_cast<const unsigned char*>(p.links) + (size_t)parity * vh * (LW * 4);
-    const unsigned char* __restrict__ xv = static_cast<const unsigned char*>(p.x);
-    const unsigned char* __restrict__ yv = static_cast<const unsigned char*>(p.r0);
-    const uint32_t* __restrict__ nbr = p.nbr + (size_t)parity * vh * 8;
-    uint32_t* __restrict__ out = static_cast<uint32_t*>(p.out);
-
-    uint32_t* stage = reinterpret_cast<uint32_t*>(tsm) + (size_t)warp * NST * STW;
-    const uint32_t stage_s = lsmem(stage);
-    const int nbl = lane >> 2;                   // the neighbour block this lane copies
-    const uint32_t nboff = (uint32_t)(lane & 3) * 16;
-    // copies of `site` (neighbour nbi of this lane's block) into stage k, as one commit group
-    auto issue = [&](int k, uint32_t site, uint32_t nbi) {
-        const uint32_t dst = stage_s + (uint32_t)k * (STW * 4);
-        const unsigned char* src = in + (size_t)nbi * SBY + nboff;
-        const uint32_t d0 = dst + (uint32_t)nbl * SBY + nboff;
-#pragma unroll
-        for (int j = 0; j < NCH; ++j) lcp16(d0 + 64 * j, src + 64 * j);
-#pragma unroll
-        for (int j = 0; j < EJ; ++j) {
-            const int e = lane + 32 * j;
-            if (e < LCH) {
-                lcp16(dst + 8 * SBY + 16 * e, lbase + (size_t)site * (LW * 4) + 16 * e);
-            } else if (e < ECH) {
-                const int e2 = e - LCH;
-                const int which = e2 >= XCH;     // 0: x, 1: r0
-                const int off = e2 - which * XCH;
-                lcp16(dst + 8 * SBY + LW * 4 + which * SBY + 16 * off,
-                      (which ? yv : xv) + (size_t)site * SBY + 16 * off);
-            }
-        }
-    };
-
-    float2 red[NTC][NVR];
-#pragma unroll
-    for (int n = 0; n < NTC; ++n)
-#pragma unroll
-        for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
-
-    const uint32_t gw = blockIdx.x * kTWarps + warp;
-    const uint32_t nw = gridDim.x * kTWarps;
-    // prologue: the first NST - 1 sites (one commit group per site slot, empty past the end)
-    uint32_t pre = gw;
-#pragma unroll
-    for (int k = 0; k < NST - 1; ++k, pre += nw) {
-        if (pre < vh) issue(k, pre, __ldg(nbr + (size_t)pre * 8 + nbl));
-        lcp_commit();
-    }
-    // neighbour index of the next site to issue, loaded one site ahead
-    uint32_t nb_next = pre < vh ? __ldg(nbr + (size_t)pre * 8 + nbl) : 0u;
-    int k = 0;                                   // stage of the current site
-    for (uint32_t site = gw; site < vh; site += nw) {
-        const uint32_t nxt = site + (NST - 1) * nw;
-        if (nxt < vh) {   // its stage was released by the __syncwarp that ended the last site
-            issue(k == 0 ? NST - 1 : k - 1, nxt, nb_next);
-            nb_next = nxt + nw < vh ? __ldg(nbr + (size_t)(nxt + nw) * 8 + nbl) : 0u;
-        }
-        lcp_commit();
-        lcp_wait<NST - 1>();                     // this lane's copies of `site` have landed
-        __syncwarp();                            // ... and every lane's
-        const uint32_t* sb = stage + k * STW;       // neighbour blocks
-        const uint32_t* lk = sb + 8 * SW + lo;      // links
-        const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
-        k = k + 1 == NST ? 0 : k + 1;
-        float Qxy[NTC][4], Qzt[NTC][4];
-#pragma unroll
-        for (int n = 0; n < NTC; ++n)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
-        uint32_t A[4];
-        mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
-        mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
-                                  m1f, m1b);
-#pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            Qxy[n][0] *= fl;
-            Qxy[n][2] *= fl;
-        }
-        mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
-        mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u);
-        mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
-        mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
-                                  m2f, m2b);
-#pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            Qzt[n][1] *= fl;
-            Qzt[n][3] *= fl;
-        }
-        mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
-        mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
-                                  0u, 0u);
-        const size_t ob = (size_t)site * SW + os;
-#pragma unroll
-        for (int n = 0; n < NTC; ++n) {
-            float2 ov[2];
-            ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
-            ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
-            ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
-            ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
-            if constexpr (EPI == EPI_PLAIN) {
-                const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
-                if (sok) {
-                    out[ob + 4 * n] = w0;
-                    out[ob + 4 * n + osn] = w1;
-                }
-            } else if (sok) {
-                const float a = (float)p.a;
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const uint32_t xw = ep[4 * n + (e ? osn : 0)];
-                    const float2 xx = M::unpack(xw);
-                    float2 res;
-                    if (EPI == EPI_XPAY) {
-                        res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
-                    } else if (EPI == EPI_RESID) {
-                        const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
-                        res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
-                    } else {
-                        res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
-                    }
-                    const uint32_t rs = M::pack(res.x, res.y);
-                    out[ob + 4 * n + (e ? osn : 0)] = rs;
-                    if constexpr (NV > 0) {
-                        const float2 rr = M::unpack(rs);
-                        if (EPI == EPI_RESID) {
-                            red[n][0].x += rr.x * rr.x + rr.y * rr.y;
-                        } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
-                            const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
-                            red[n][0].x += qq.x * rr.x + qq.y * rr.y;
-                            red[n][0].y += qq.x * rr.y - qq.y * rr.x;
-                        } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
-                            red[n][0].x += rr.x * xx.x + rr.y * xx.y;
-                            red[n][0].y += rr.x * xx.y - rr.y * xx.x;
-                            red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
-                        }
-                    }
-                }
-            }
-        }
-        __syncwarp();   // every lane has read this stage before it is refilled
-    }
-    lcp_wait<0>();      // no copy outlives the kernel (only empty groups remain at this point)
-    if constexpr (NV > 0) {
-        __shared__ double2 wsum[kTWarps][NV][kLMaxChunkRhs];
-        __shared__ double2 bsum[NV * kMaxRhs];
-#pragma unroll
-        for (int n = 0; n < NTC; ++n)
-#pragma unroll
-            for (int kk = 0; kk < NV; ++kk) {
-                double vx = (double)red[n][kk].x, vy = (double)red[n][kk].y;
-#pragma unroll
-                for (int off = 4; off < 32; off <<= 1) {
-                    vx += __shfl_xor_sync(0xffffffffu, vx, off);
-                    vy += __shfl_xor_sync(0xffffffffu, vy, off);
-                }
-                if (g == 0) wsum[warp][kk][4 * n + t] = make_double2(vx, vy);
-            }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < NV * MR; idx += blockDim.x) {
-            const int kk = idx / MR, rhs = idx - kk * MR;
-            double2 s = make_double2(0.0, 0.0);
-            for (int w = 0; w < kTWarps; ++w) {
-                s.x += wsum[w][kk][rhs].x;
-                s.y += wsum[w][kk][rhs].y;
-            }
-            bsum[idx] = s;
-        }
-        __syncthreads();
-        publish_and_finish<NV>(bsum, MR, p.red);
-    }
-}
-
-template <typename S, int NC, int NTC, int EPI, bool DAG>
-void* async_kernel_ptr() {
-    return reinterpret_cast<void*>(hop_mmal_async_kernel<S, NC, DAG, EPI, NTC>);
-}
-
-template <typename S, int NC, int NTC>
-int launch_mmal_async(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
-    void (*k)(const HopParams) = nullptr;
-    switch (epi) {
-        case EPI_PLAIN: k = dagger ? hop_mmal_async_kernel<S, NC, true, EPI_PLAIN, NTC> : hop_mmal_async_kernel<S, NC, false, EPI_PLAIN, NTC>; break;
-        case EPI_XPAY: k = dagger ? hop_mmal_async_kernel<S, NC, true, EPI_XPAY, NTC> : hop_mmal_async_kernel<S, NC, false, EPI_XPAY, NTC>; break;
-        case EPI_SCHUR_R0: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR_R0, NTC>; break;
-        case EPI_SCHUR_TS: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR_TS, NTC>; break;
-        case EPI_SCHUR: k = hop_mmal_async_kernel<S, NC, false, EPI_SCHUR, NTC>; break;
-        case EPI_RESID: k = hop_mmal_async_kernel<S, NC, false, EPI_RESID, NTC>; break;
-        default: return set_error(QCU_ERR_INVALID, "epilogue %d", epi);
-    }
-    const int nx = epi == EPI_PLAIN ? 0 : ((epi == EPI_SCHUR_R0 || epi == EPI_RESID) ? 2 : 1);
-    const size_t smem = (size_t)kTWarps * astages(NC, 4 * NTC, nx) * tstage_bytes(NC, 4 * NTC, nx);
-    int grid = resident_grid(k, kTThreads, p.g.vh * 32, smem);
-    if (grid > kScratchBlocks) grid = kScratchBlocks;
-    k<<<grid, kTThreads, smem, st>>>(p);
-    QCUB_CHECK_LAUNCH();
-    return QCU_SUCCESS;
 }
 
 template <typename S, int NC, int NTC, int EPI, bool DAG>
@@ -915,8 +662,7 @@ int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, cudaStre
     if (pre && nchunk == 1 && p.m == 4 * NTC && lalign16(p.in) && lalign16(p.links) &&
         (!p.x || lalign16(p.x)) && (!p.r0 || lalign16(p.r0)))
     {
-        if (std::getenv("QCU_XP_TMA")) return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
-        return launch_mmal_async<S, NC, NTC>(p, dagger, epi, st);
+        return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
     }
     if (p.m == 4 * NTC * nchunk)
         return pre ? launch_mmal_t<S, NC, NTC, true, true>(p, dagger, epi, nchunk, st)
@@ -961,17 +707,6 @@ cudaError_t mmal_tma_optin() {
                          tma_kernel_ptr<S, NC, NTC, EPI_SCHUR, false>(), tma_kernel_ptr<S, NC, NTC, EPI_RESID, false>()};
     for (const void* k : ks) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
-        if (e != cudaSuccess) return e;
-    }
-    const void* ak[8] = {async_kernel_ptr<S, NC, NTC, EPI_PLAIN, false>(), async_kernel_ptr<S, NC, NTC, EPI_PLAIN, true>(),
-                         async_kernel_ptr<S, NC, NTC, EPI_XPAY, false>(), async_kernel_ptr<S, NC, NTC, EPI_XPAY, true>(),
-                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR_R0, false>(),
-                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR_TS, false>(),
-                         async_kernel_ptr<S, NC, NTC, EPI_SCHUR, false>(), async_kernel_ptr<S, NC, NTC, EPI_RESID, false>()};
-    int aneed = 0;
-    for (int nx = 0; nx <= 2; ++nx) aneed = std::max(aneed, kTWarps * astages(NC, 4 * NTC, nx) * tstage_bytes(NC, 4 * NTC, nx));
-    for (const void* k : ak) {
-        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, aneed);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -149,6 +149,25 @@ __device__ __forceinline__ uint32_t lproject(uint32_t pw, uint32_t qw, uint32_t 
     return M::fma(qw, unit_pair<S>(SG, SG), pw);
 }
 
+// Groups of 4 RHS (the 4 B columns pairs of one MMA) that a work unit computes: bit n for
+// group n (RHS rb0 + 4n .. rb0 + 4n + 3) if it holds an RHS below m and, when per-RHS
+// activity flags are given, at least one active RHS.  Warp-uniform.
+template <int NTC>
+__device__ __forceinline__ uint32_t active_groups(const int* __restrict__ active, int rb0, int m) {
+    uint32_t gm = 0u;
+#pragma unroll
+    for (int n = 0; n < NTC; ++n) {
+        const int r0 = rb0 + 4 * n;
+        if (r0 >= m) break;
+        bool on = active == nullptr;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (!on && r0 + r < m) on = __ldg(active + r0 + r) != 0;
+        if (on) gm |= 1u << n;
+    }
+    return gm;
+}
+
 // A fragment of direction MU.  Rows are ordered (re/im, sum/diff, colour): lane (g, t) holds
 // rows g (re) and g + 8 (im) of class cls = g / 4 (0 sum, 1 diff) and colour g % 4, for
 // K slots t (forward colour t) and t + 4 (backward colour t).  wf = W_f[g%4][t] (t-boundary

@@ -43,13 +43,13 @@ __device__ __forceinline__ void mmalb_dir(float (&Sq)[NTC][4], float (&Q)[NTC][4
                                           const uint32_t* __restrict__ bw, int o0, int o4, int c0, int c4,
                                           const uint32_t (&As0)[4], const uint32_t (&As1)[4],
                                           const uint32_t (&Ad0)[4], const uint32_t (&Ad1)[4], uint32_t lmf,
-                                          uint32_t lmb, int rb0, int q, int m) {
+                                          uint32_t lmb, int rb0, int q, int m, uint32_t gmask) {
     using M = LMma<S>;
     constexpr int SB = -SF;
     uint32_t w[NTC][8];
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
+        if (!((gmask >> n) & 1u)) continue;   // warp-uniform: absent or inactive group
         int d = 4 * n;
         if (!EXACT) d += min(0, m - 1 - (rb0 + 4 * n + q));
         w[n][0] = __ldg(fw + o0 + d);
@@ -63,7 +63,7 @@ __device__ __forceinline__ void mmalb_dir(float (&Sq)[NTC][4], float (&Q)[NTC][4
     }
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!EXACT && rb0 + 4 * n >= m) break;
+        if (!((gmask >> n) & 1u)) continue;
         const uint32_t hf0 = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
         const uint32_t hf4 = lproject<S, MU, SF>(w[n][2], w[n][3], lmf);
         const uint32_t hb0 = lproject<S, MU, SB>(w[n][4], w[n][5], lmb);
@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(kLThreads, 2) hop_mmal_big_kernel(const HopPar
     const uint32_t site_stride = (uint32_t)(nw / nchunk);
     const uint32_t site0 = gw < (int64_t)site_stride * nchunk ? (uint32_t)(gw / nchunk) : vh;
     const int rb0 = chunk * NTC * 4;
+    const uint32_t gmask = active_groups<NTC>(p.active, rb0, m);
     const uint32_t* __restrict__ in = static_cast<const uint32_t*>(p.in) + rb0 + q;
 
     float2 red[NTC][NVR];
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(kLThreads, 2) hop_mmal_big_kernel(const HopPar
             for (int n = 0; n < NTC; ++n) {
 #pragma unroll
                 for (int e = 0; e < 4; ++e) xw[n][e] = yw[n][e] = 0u;
-                if (!EXACT && rb0 + 4 * n >= m) break;
+                if (!((gmask >> n) & 1u)) continue;
                 if (sok && (EXACT || rb0 + 4 * n + t < m)) {
                     const size_t o = sbase + os + 4 * n;
 #pragma unroll
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(kLThreads, 2) hop_mmal_big_kernel(const HopPar
         bemb(Ad0, wphase<LRecon<MU, SF>::C2>(wf0[MU]), wphase<LRecon<MU, SF>::C2>(wf4[MU]));                  \
         bemb(Ad1, wphase<LRecon<MU, SF>::C2 ^ 1>(wb0[MU]), wphase<LRecon<MU, SF>::C2 ^ 1>(wb4[MU]));          \
         mmalb_dir<S, MU, SF, NTC, EXACT>(Sq, Q, in + (size_t)(FNB) * SW, in + (size_t)(BNB) * SW, o0, o4, C0, C4, \
-                                         As0, As1, Ad0, Ad1, LMF, LMB, rb0, q, m)
+                                         As0, As1, Ad0, Ad1, LMF, LMB, rb0, q, m, gmask)
         // y, then spin 3 (diff column h0: registers 0 and 2) negated, then x; z, then spin 3
         // (column h1: registers 1 and 3) negated, then t
         QCUB_BIG_DIR(1, Qxy, nb[2], nb[3], c01_0, c01_4, m1f, m1b);
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(kLThreads, 2) hop_mmal_big_kernel(const HopPar
 
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
-            if (!EXACT && rb0 + 4 * n >= m) break;
+            if (!((gmask >> n) & 1u)) continue;
             const bool rok = sok && (EXACT || rb0 + 4 * n + t < m);
             const size_t o = sbase + os + 4 * n;
             float2 ov[4];

@@ -36,6 +36,7 @@ struct Hop {
     const void* gauge;
     const void* links = nullptr;   // per-site tables of the tensor-core hop (or null)
     const uint32_t* nbr = nullptr;
+    const int* active = nullptr;   // per-RHS activity flags (device), or null: all RHS
     // fetch (build on first use) the per-site tables when the hop kernel for this shape
     // reads them; call outside graph capture
     int tables() {
@@ -61,6 +62,7 @@ struct Hop {
         p.gate = gate;
         p.links = links;
         p.nbr = nbr;
+        p.active = active;
         return hop_launch(p, c.nc, prec, false, epi, c.stream);
     }
 };
@@ -357,7 +359,10 @@ int SchurSolve::enqueue_iteration() {
     const int* gate = &dsc_->gate;
     const int XP = QCU_PRECISION_SINGLE;
     Hop h64{c, P_, g_};
-    Hop hs{c, S_, gs_, links_s_, nbr_s_};
+    // sloppy hops skip the groups of 4 RHS whose FP64 residual has converged: the reliable
+    // update clears their flags, their scalars are 0 from then on, so their sloppy vectors
+    // keep finite values that no update uses
+    Hop hs{c, S_, gs_, links_s_, nbr_s_, dsc_->active};
     // sloppy BiCGStab iteration
     if ((e = hs.launch(tmps, ps, 0, EPI_PLAIN, nullptr, nullptr, 0.0, FIN_NONE, nullptr, nullptr, done))) return e;
     if ((e = hs.launch(vs, tmps, 1, EPI_SCHUR_R0, ps, r0s, k2, FIN_ALPHA, dsc_, dsc_->red[0], done))) return e;

@@ -5,6 +5,7 @@ import ctypes
 
 import numpy as np
 import pytest
+import torch
 
 import qcu_mrhs_b200 as q
 from qcu_mrhs_b200 import fields as F
@@ -142,7 +143,7 @@ def test_start_dslash_and_mat_low_precision_tables(oracle_lib, prec, t_boundary,
 @pytest.mark.parametrize("m", [4, 8, 12, 16, 6])
 def test_context_hop(oracle_lib, prec, m):
     """qcuDslashMrhsContext: the context's own hop (gauge copy, t boundary, and for FP16/BF16
-    the per-site tables; m = 4, 8, 12, 16 run the bulk-copy staged tensor-core kernel) on
+    the per-site tables; m = 4, 8, 12, 16 run the shared-memory staged tensor-core kernel) on
     caller gathered fields, both parities and dagger, against the oracle on the same
     rounded inputs; the same call twice gives the same bits (the tables are reused)."""
     L, nc, kappa = (8, 4, 4, 6), 3, 0.11
@@ -166,6 +167,128 @@ def test_context_hop(oracle_lib, prec, m):
             q.check(q.lib().qcuDslashMrhsContext(d_out2.data_ptr(), d_in.data_ptr(), parity, dagger, prec, None))
             sync()
             assert np.array_equal(got, from_dev(d_out2))
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
+@pytest.mark.parametrize("nc,m,flags", [
+    (3, 12, [1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0]),   # staged kernel: group 1 inactive
+    (3, 16, [0, 0, 0, 0, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 1]),   # groups 0 and 2 inactive
+    (3, 7, [1, 1, 0, 1, 0, 0, 0]),                   # generic kernel, partial group 1 inactive
+    (6, 8, [0, 0, 0, 0, 0, 1, 0, 0]),                # N = 6 kernel: group 0 inactive
+])
+@pytest.mark.parametrize("prec", [q.HALF, q.BF16])
+def test_context_hop_skips_inactive_groups(oracle_lib, prec, nc, m, flags):
+    """qcuDslashMrhsContextActive with the tensor-core hop: groups of 4 RHS whose flags are
+    all 0 keep the output buffer's previous contents bit for bit, every other group is
+    bit-identical to the hop without flags."""
+    L, kappa = (8, 4, 4, 6), 0.11
+    gauge, dg = _setup(L, nc, m, kappa, 33)
+    o = q.default_options()
+    o.t_boundary = -1.0
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    q.check(q.lib().qcuSetHopKernel(q.HOP_MMA_LINK))
+    try:
+        inp = F.to_mrhs(F.gaussian_fermions(L, nc, m, 34, parities=1)[:, 0])
+        old = F.to_mrhs(F.gaussian_fermions(L, nc, m, 35, parities=1)[:, 0])
+        d_in = to_dev(inp, prec)
+        d_act = torch.tensor(flags, dtype=torch.int32, device="cuda")
+        for parity in (0, 1):
+            d_full = empty_dev(inp.shape, prec)
+            q.check(q.lib().qcuDslashMrhsContext(d_full.data_ptr(), d_in.data_ptr(), parity, 0, prec, None))
+            d_out = to_dev(old, prec)
+            q.check(q.lib().qcuDslashMrhsContextActive(d_out.data_ptr(), d_in.data_ptr(), parity, 0, prec,
+                                                        d_act.data_ptr(), None))
+            sync()
+            full, got, before = from_dev(d_full), from_dev(d_out), from_dev(to_dev(old, prec))
+            for g0 in range(0, m, 4):
+                sl = slice(g0, min(g0 + 4, m))
+                if any(flags[sl]):
+                    assert np.array_equal(got[..., sl], full[..., sl]), (parity, g0)
+                else:
+                    assert np.array_equal(got[..., sl], before[..., sl]), (parity, g0)
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
+def test_context_hop_with_half_the_groups_inactive_is_faster():
+    """The cost of the skipped groups: FP16, 24^3 x 48, N = 3, m = 8, tensor-core hop, CUDA
+    events over 20 launches after 3 warm-up; with group 1 (RHS 4-7) inactive the hop skips
+    that group's neighbour and epilogue copies and all of its MMAs, so it must take clearly
+    less time than with both groups live."""
+    L, nc, m, kappa = (24, 24, 24, 48), 3, 8, 0.124
+    init(L, nc, m)
+    vh = F.half_volume(L)
+    dg = torch.randn((4, 2, vh, nc, nc, 2), device="cuda", dtype=torch.float64)   # timing only
+    q.lib().loadQcuGauge(dg.data_ptr(), q.DOUBLE)
+    q.lib().getDslash(0, 1.0 / (2 * kappa) - 4.0)
+    q.check()
+    q.check(q.lib().qcuSetHopKernel(q.HOP_MMA_LINK))
+    try:
+        d_in = torch.randn((vh, 4, nc, m, 2), device="cuda").to(torch.float16)
+        d_out = torch.empty_like(d_in)
+        masks = {"all": [1] * 8, "half": [1, 1, 1, 1, 0, 0, 0, 0]}
+        times = {}
+        for name, fl in masks.items():
+            act = torch.tensor(fl, dtype=torch.int32, device="cuda")
+            for _ in range(3):
+                q.check(q.lib().qcuDslashMrhsContextActive(d_out.data_ptr(), d_in.data_ptr(), 0, 0, q.HALF,
+                                                            act.data_ptr(), None))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for i in range(20):
+                q.lib().qcuDslashMrhsContextActive(d_out.data_ptr(), d_in.data_ptr(), i & 1, 0, q.HALF,
+                                                   act.data_ptr(), None)
+            e1.record()
+            torch.cuda.synchronize()
+            q.check()
+            times[name] = e0.elapsed_time(e1) / 20
+        print("hop ms", times)
+        assert times["half"] <= 0.85 * times["all"], times
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
+
+
+def test_mixed_solve_drops_converged_rhs_groups(oracle_lib):
+    """Mixed FP16 solve with the tensor-core sloppy hop where one group of 4 RHS is
+    converged from the start (zero sources, as when a batch is padded to a multiple of 4):
+    the sloppy hops skip that group, its solutions are exactly 0, and the live RHS reach the
+    FP64 true-residual tolerance as when solved next to live partners."""
+    L, nc, m, kappa, tol = (8, 4, 4, 8), 3, 8, 0.11, 1e-10
+    gauge, dg = _setup(L, nc, m, kappa, 71, kind="smooth")
+    vh = F.half_volume(L)
+    o = q.default_options()
+    o.solver = q.SOLVER_MIXED
+    o.sloppy_precision = q.HALF
+    o.stop_true_residual = 1
+    o.t_boundary = -1.0
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    q.check(q.lib().qcuSetHopKernel(q.HOP_MMA_LINK))
+    try:
+        b_live = F.gaussian_fermions(L, nc, m, 72)
+        runs = {}
+        for name in ("padded", "live"):
+            b = b_live.copy()
+            if name == "padded":
+                b[4:] = 0
+            ins = [to_dev(b[j]) for j in range(m)]
+            outs = [empty_dev((2, vh, 4, nc)) for _ in range(m)]
+            for j in range(m):
+                q.lib().pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
+            q.lib().qcuInvert(2000, tol)
+            assert q.status() == q.SUCCESS, q.last_error()
+            x = np.stack([from_dev(v) for v in outs])
+            runs[name] = (b, x, q.solve_stats().iterations)
+        b, x, it_padded = runs["padded"]
+        assert np.all(x[4:] == 0)
+        res = oracle_lib.mat(x[:4], gauge, L, kappa, t_sign=-1.0) - b[:4]
+        rel = np.linalg.norm(res.reshape(4, -1), axis=1) / np.linalg.norm(b[:4].reshape(4, -1), axis=1)
+        assert np.all(rel <= 2 * tol), rel
+        # the live group alone needs no more iterations than next to live partners
+        assert it_padded <= runs["live"][2] + 3, (it_padded, runs["live"][2])
+    finally:
+        q.lib().qcuSetHopKernel(q.HOP_AUTO)
     assert q.lib().qcuGetKernelError(1) == 0
 
 
