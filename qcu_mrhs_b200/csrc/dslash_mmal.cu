@@ -336,24 +336,25 @@ __device__ __forceinline__ bool lbar_wait(uint32_t bar, uint32_t parity) {
 // Bytes of one stage: 8 neighbour blocks, the link block, NX epilogue blocks.
 __host__ __device__ constexpr int tstage_bytes(int nc, int m, int nx) { return (8 + nx) * 16 * nc * m + 32 * nc * nc; }
 
-template <typename S, int MU, int SF, int NTC>
-__device__ __forceinline__ void mmal_dir_s(float (&Q)[NTC][4], const uint32_t* pf, const uint32_t* qf,
+// One direction of the staged kernel for NT tiles: tile n takes the group of 4 RHS at word
+// offset go(n) of a spin-colour row (4 n when all groups are live, DENSE).
+template <typename S, int MU, int SF, int NT, bool DENSE>
+__device__ __forceinline__ void mmal_dir_s(float (&Q)[NT][4], const uint32_t* pf, const uint32_t* qf,
                                            const uint32_t* pb, const uint32_t* qb, const uint32_t (&A)[4],
-                                           uint32_t lmf, uint32_t lmb, uint32_t gmask) {
+                                           uint32_t lmf, uint32_t lmb, const int (&go)[NT]) {
     using M = LMma<S>;
     constexpr int SB = -SF;
-    uint32_t w[NTC][4];
+    uint32_t w[NT][4];
 #pragma unroll
-    for (int n = 0; n < NTC; ++n) {
-        if (!((gmask >> n) & 1u)) continue;   // warp-uniform: inactive group
-        w[n][0] = pf[4 * n];
-        w[n][1] = qf[4 * n];
-        w[n][2] = pb[4 * n];
-        w[n][3] = qb[4 * n];
+    for (int n = 0; n < NT; ++n) {
+        const int o = DENSE ? 4 * n : go[n];
+        w[n][0] = pf[o];
+        w[n][1] = qf[o];
+        w[n][2] = pb[o];
+        w[n][3] = qb[o];
     }
 #pragma unroll
-    for (int n = 0; n < NTC; ++n) {
-        if (!((gmask >> n) & 1u)) continue;
+    for (int n = 0; n < NT; ++n) {
         const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
         const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
         M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
@@ -451,12 +452,25 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
 #pragma unroll
         for (int k = 0; k < NVR; ++k) red[n][k] = make_float2(0.f, 0.f);
 
-    // the warp's sites; MASKED: some group of 4 RHS is inactive.  Both forms are compiled so
-    // that the all-active case keeps straight-line code (no per-group branches between the
-    // loads of successive groups).
-    auto sites = [&](auto masked) {
-        constexpr bool MASKED = decltype(masked)::value;
-        const uint32_t gm = MASKED ? gmask : (1u << NTC) - 1u;
+    // Live groups: the warp computes NA = popcount(gmask) tiles, tile n on the n-th live
+    // group (groups in order).  Each NA is compiled separately, so every form is
+    // straight-line code and the all-live form (NA = NTC) has compile-time offsets.
+    const int na = __popc(gmask);
+    auto sites = [&](auto na_tag) {
+        constexpr int NA = decltype(na_tag)::value;
+        constexpr bool DENSE = NA == NTC;
+        int go[NA];   // word offset of tile n's group: the n-th set bit of gmask, times 4
+        uint32_t rest = gmask;
+#pragma unroll
+        for (int n = 0; n < NA; ++n) {
+            go[n] = 4 * (__ffs(rest) - 1);
+            rest &= rest - 1u;
+        }
+        float2 rt[NA][NVR];   // this form's partial sums per tile
+#pragma unroll
+        for (int n = 0; n < NA; ++n)
+#pragma unroll
+            for (int kk = 0; kk < NVR; ++kk) rt[n][kk] = make_float2(0.f, 0.f);
         uint32_t site = gw;
         uint32_t inflight = 0;   // bit k: stage k has copies in flight
         uint32_t use = 0;        // uses of each stage so far (bit k = parity of stage k's next wait)
@@ -484,37 +498,37 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
             const uint32_t* sb = stage + k * STW;       // neighbour blocks
             const uint32_t* lk = sb + 8 * SW + lo;      // links
             const uint32_t* ep = sb + 8 * SW + LW + os; // x, then r0
-            float Qxy[NTC][4], Qzt[NTC][4];
+            float Qxy[NA][4], Qzt[NA][4];
 #pragma unroll
-            for (int n = 0; n < NTC; ++n)
+            for (int n = 0; n < NA; ++n)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) Qxy[n][e] = Qzt[n][e] = 0.f;
             uint32_t A[4];
             mmal_a(A, lk[2 * N2], lk[3 * N2], okm, ph1.sel, ph1.mf, ph1.mb);
-            mmal_dir_s<S, 1, SF, NTC>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
-                                      m1f, m1b, gm);
+            mmal_dir_s<S, 1, SF, NA, DENSE>(Qxy, sb + 2 * SW + oa, sb + 2 * SW + ob01, sb + 3 * SW + oa, sb + 3 * SW + ob01, A,
+                                      m1f, m1b, go);
 #pragma unroll
-            for (int n = 0; n < NTC; ++n) {
+            for (int n = 0; n < NA; ++n) {
                 Qxy[n][0] *= fl;
                 Qxy[n][2] *= fl;
             }
             mmal_a(A, lk[0], lk[N2], okm, ph0.sel, ph0.mf, ph0.mb);
-            mmal_dir_s<S, 0, SF, NTC>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u, gm);
+            mmal_dir_s<S, 0, SF, NA, DENSE>(Qxy, sb + oa, sb + ob01, sb + SW + oa, sb + SW + ob01, A, 0u, 0u, go);
             mmal_a(A, lk[4 * N2], lk[5 * N2], okm, ph2.sel, ph2.mf, ph2.mb);
-            mmal_dir_s<S, 2, SF, NTC>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
-                                      m2f, m2b, gm);
+            mmal_dir_s<S, 2, SF, NA, DENSE>(Qzt, sb + 4 * SW + oa, sb + 4 * SW + ob23, sb + 5 * SW + oa, sb + 5 * SW + ob23, A,
+                                      m2f, m2b, go);
 #pragma unroll
-            for (int n = 0; n < NTC; ++n) {
+            for (int n = 0; n < NA; ++n) {
                 Qzt[n][1] *= fl;
                 Qzt[n][3] *= fl;
             }
             mmal_a(A, lk[6 * N2], lk[7 * N2], okm, ph3.sel, ph3.mf, ph3.mb);
-            mmal_dir_s<S, 3, SF, NTC>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
-                                      0u, 0u, gm);
+            mmal_dir_s<S, 3, SF, NA, DENSE>(Qzt, sb + 6 * SW + oa, sb + 6 * SW + ob23, sb + 7 * SW + oa, sb + 7 * SW + ob23, A,
+                                      0u, 0u, go);
             const size_t ob = (size_t)site * SW + os;
 #pragma unroll
-            for (int n = 0; n < NTC; ++n) {
-                if (!((gm >> n) & 1u)) continue;
+            for (int n = 0; n < NA; ++n) {
+                const int gn = DENSE ? 4 * n : go[n];   // word offset of the tile's group
                 float2 ov[2];
                 ov[0].x = Qzt[n][0] + (cls ? Qxy[n][1] : Qxy[n][0]);
                 ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
@@ -523,38 +537,38 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
                 if constexpr (EPI == EPI_PLAIN) {
                     const uint32_t w0 = M::pack(ov[0].x, ov[0].y), w1 = M::pack(ov[1].x, ov[1].y);
                     if (sok) {
-                        out[ob + 4 * n] = w0;
-                        out[ob + 4 * n + osn] = w1;
+                        out[ob + gn] = w0;
+                        out[ob + gn + osn] = w1;
                     }
                 } else if (sok) {
                     const float a = (float)p.a;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
-                        const uint32_t xw = ep[4 * n + (e ? osn : 0)];
+                        const uint32_t xw = ep[gn + (e ? osn : 0)];
                         const float2 xx = M::unpack(xw);
                         float2 res;
                         if (EPI == EPI_XPAY) {
                             res = make_float2(xx.x + a * ov[e].x, xx.y + a * ov[e].y);
                         } else if (EPI == EPI_RESID) {
-                            const float2 yy = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
+                            const float2 yy = M::unpack(ep[SW + gn + (e ? osn : 0)]);
                             res = make_float2(yy.x - xx.x + a * ov[e].x, yy.y - xx.y + a * ov[e].y);
                         } else {
                             res = make_float2(xx.x - a * ov[e].x, xx.y - a * ov[e].y);
                         }
                         const uint32_t rs = M::pack(res.x, res.y);
-                        out[ob + 4 * n + (e ? osn : 0)] = rs;
+                        out[ob + gn + (e ? osn : 0)] = rs;
                         if constexpr (NV > 0) {
                             const float2 rr = M::unpack(rs);
                             if (EPI == EPI_RESID) {
-                                red[n][0].x += rr.x * rr.x + rr.y * rr.y;
+                                rt[n][0].x += rr.x * rr.x + rr.y * rr.y;
                             } else if (EPI == EPI_SCHUR_R0) {   // <r0, out> = sum conj(r0) out
-                                const float2 qq = M::unpack(ep[SW + 4 * n + (e ? osn : 0)]);
-                                red[n][0].x += qq.x * rr.x + qq.y * rr.y;
-                                red[n][0].y += qq.x * rr.y - qq.y * rr.x;
+                                const float2 qq = M::unpack(ep[SW + gn + (e ? osn : 0)]);
+                                rt[n][0].x += qq.x * rr.x + qq.y * rr.y;
+                                rt[n][0].y += qq.x * rr.y - qq.y * rr.x;
                             } else if (EPI == EPI_SCHUR_TS) {  // <out, x>, <out, out>
-                                red[n][0].x += rr.x * xx.x + rr.y * xx.y;
-                                red[n][0].y += rr.x * xx.y - rr.y * xx.x;
-                                red[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
+                                rt[n][0].x += rr.x * xx.x + rr.y * xx.y;
+                                rt[n][0].y += rr.x * xx.y - rr.y * xx.x;
+                                rt[n][NV - 1].x += rr.x * rr.x + rr.y * rr.y;
                             }
                         }
                     }
@@ -570,11 +584,27 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
                     if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) break;
                 }
         }
+        // partial sums back to their groups
+#pragma unroll
+        for (int n = 0; n < NA; ++n)
+#pragma unroll
+            for (int gi = 0; gi < NTC; ++gi)
+                if ((DENSE ? 4 * n : go[n]) == 4 * gi)
+#pragma unroll
+                    for (int kk = 0; kk < NVR; ++kk) {
+                        red[gi][kk].x += rt[n][kk].x;
+                        red[gi][kk].y += rt[n][kk].y;
+                    }
     };
-    if (gmask == (1u << NTC) - 1u)
-        sites(std::false_type{});
-    else
-        sites(std::true_type{});
+    if (na == NTC) {
+        sites(std::integral_constant<int, NTC>{});
+    } else if (na == 1) {
+        if constexpr (NTC > 1) sites(std::integral_constant<int, 1>{});
+    } else if (na == 2) {
+        if constexpr (NTC > 2) sites(std::integral_constant<int, 2>{});
+    } else if (na == 3) {
+        if constexpr (NTC > 3) sites(std::integral_constant<int, 3>{});
+    }   // na == 0: nothing to compute, the outputs stay as they were
 
     if constexpr (NV > 0) {
         __shared__ double2 wsum[kTWarps][NV][kLMaxChunkRhs];

