@@ -54,6 +54,8 @@ CHECK_INTERVAL = 16
 MEASURED_TRAFFIC = {("f16", "packed16_pairs"): 490.7e6, ("f16", "packed16"): 530.2e6, ("f16", "simt"): 610.6e6}
 # arithmetic of each 16-bit hop kernel
 DTYPE_DETAIL = {
+    "mma_link_direct": "FP16 storage; spin projection in FP16 (one rounding), link products and the sum of the 8 "
+                       "hops in FP32 on the tensor cores (mma.sync m16n8k16, FP32 accumulate)",
     "mma_link": "FP16 storage; spin projection in FP16 (one rounding), link products and the sum of the 8 hops "
                 "in FP32 on the tensor cores (mma.sync m16n8k16, FP32 accumulate)",
     "packed16_pairs": "FP16 storage; projection and the 3-term colour sums of each link product in packed FP16, "
@@ -273,7 +275,8 @@ def main():
 
     # hop kernel per (N, m, precision) picked by the autotuner before anything is timed
     tuned = {}
-    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16", 9: "mma_link"}
+    names = {1: "simt", 2: "tcgen05", 3: "simt_cs", 4: "packed16", 7: "packed16_pairs", 8: "mma16", 9: "mma_link",
+             10: "mma_link_direct"}
     for name, prec in (("f64", q.DOUBLE), ("f16", q.HALF), ("bf16", q.BF16)):
         if args.static_kernels:
             k = lib.qcuGetAutoHop(NC, M, prec)    # the static rule (nothing recorded)
@@ -410,7 +413,32 @@ def main():
                       "launch_us": dur * 1e6,
                       "algorithmic_bytes": byts, "gflops": hop_flops(vh, NC, M) / dur / 1e9,
                       "kernel": tuned[name], "peak_kind": f"{peak_kind} HBM copy bandwidth"}
-        del a, out
+        # the two Schur forms of every BiCGStab iteration (qcuDslashMrhsContextForm: the same
+        # kernels as the solver's): out = x - kappa^2 D in with the fused sums <r0, out> or
+        # <out, x>, <out, out>; their algorithmic bytes add x (and r0), each read once
+        xs = torch.randn_like(psi64).to(dt)
+        r0s = torch.randn_like(psi64).to(dt)
+        red = torch.empty((2 * M, 2), dtype=torch.float64, device="cuda")
+        spinor = vh * 4 * NC * M * 2 * s_b
+        forms = {}
+        for fname, form, extra in (("schur_r0", q.HOP_FORM_SCHUR_R0, 2), ("schur_ts", q.HOP_FORM_SCHUR_TS, 1)):
+            def run_form(i):
+                return lib.qcuDslashMrhsContextForm(out.data_ptr(), a.data_ptr(), xs.data_ptr(), r0s.data_ptr(),
+                                                    KAPPA * KAPPA, form, i & 1, prec, red.data_ptr(), dev_stream)
+            for i in range(3):
+                q.check(run_form(i))
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for i in range(reps):
+                q.check(run_form(i))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fdur = e0.elapsed_time(e1) / 1e3 / reps
+            fb = byts + extra * spinor
+            forms[fname] = {"launch_us": fdur * 1e6, "algorithmic_bytes": fb, "achieved": fb / fdur / 1e9,
+                            "frac": fb / fdur / 1e9 / hbm}
+        roof[name]["schur_forms"] = forms
+        del a, out, xs, r0s, red
     del psi64, ref_out
 
     # ---- end to end through the C ABI with host buffers ----

@@ -198,6 +198,22 @@ int qcuDslashMrhsContext(void *out, const void *in, int parity, int dagger, int 
  * mixed solver's sloppy hops run this way with the flags of its converged RHS. */
 int qcuDslashMrhsContextActive(void *out, const void *in, int parity, int dagger, int precision,
                                const int *active, void *stream);
+/* The context's hop with one of the fused epilogues its solvers run (the same kernels):
+ *   PLAIN     out = D in
+ *   XPAY      out = x + a D in
+ *   SCHUR_R0  out = x - a D in, and red[j] = <r0_j, out_j>            (BiCGStab v = A p)
+ *   SCHUR_TS  out = x - a D in, and red[j] = <out_j, x_j>, red[m + j] = <out_j, out_j>
+ *   SCHUR     out = x - a D in
+ *   RESID     out = r0 - (x - a D in), and red[j] = ||out_j||^2
+ * red: device double2 array of (number of sums) x m_rhs, or NULL to discard the sums. */
+#define QCU_HOP_FORM_PLAIN 0
+#define QCU_HOP_FORM_XPAY 1
+#define QCU_HOP_FORM_SCHUR_R0 2
+#define QCU_HOP_FORM_SCHUR_TS 3
+#define QCU_HOP_FORM_SCHUR 4
+#define QCU_HOP_FORM_RESID 5
+int qcuDslashMrhsContextForm(void *out, const void *in, const void *x, const void *r0, double a, int form,
+                             int parity, int precision, void *red, void *stream);
 
 /* Schur operator out_o = in_o - kappa^2 D_oe D_eo in_o; tmp is one half-lattice vector.
  * Replaces fused_x_sub_Doe_Deo_x -- reference src/solver/bicgstab_solve.cu:27-70. */
@@ -300,18 +316,21 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *            explicit request selects it: its Schur and residual forms, most of the
  *            solver's hops, are slower than PACKED16_PAIRS's, which the autotuner's
  *            plain-hop timing does not see;
- *   MMA_LINK FP16/BF16, 2 <= n_color <= 4, any m_rhs: one warp per (site, up to 16 RHS),
- *            the links as the A operand of mma.sync m16n8k16 and the projected neighbour
- *            half spinors (columns = RHS x half spinor) as B; the forward and backward hop
- *            of a direction are one MMA per 4 RHS, link products and the sum of the 8 hops
- *            in FP32, the spin projection the only 16-bit arithmetic.  On a context (the
- *            solvers, start_dslash, mat_Qcu, qcuDslashMrhsContext) it reads a per-site
- *            neighbour table and hop-link array, and for m_rhs = 4, 8, 12, 16 stages the
- *            neighbour and link blocks in shared memory with bulk asynchronous copies
- *            (whole rows of the half lattice per block where Lx <= 32); else as AUTO;
+ *   MMA_LINK FP16/BF16, 2 <= n_color <= 8, any m_rhs: one warp per (site, up to 16 RHS; 8
+ *            for n_color >= 5), the links as the A operand of mma.sync m16n8k16 and the
+ *            projected neighbour half spinors (columns = RHS x half spinor) as B; the
+ *            forward and backward hop of a direction are one MMA per 4 RHS (four for
+ *            n_color >= 5), link products and the sum of the 8 hops in FP32, the spin
+ *            projection the only 16-bit arithmetic.  On a context (the solvers,
+ *            start_dslash, mat_Qcu, qcuDslashMrhsContext*) it reads a per-site neighbour
+ *            table and hop-link array, and for n_color <= 4 and m_rhs = 4, 8, 12, 16 stages
+ *            each site's neighbour, link and epilogue blocks in shared memory with bulk
+ *            asynchronous copies (the TMA engine, bounded mbarrier waits);
+ *   MMA_LINK_DIRECT  the same kernels without the shared-memory staging (fragment words
+ *            loaded straight from global memory): faster where the fields stay in L2;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
- *            (n_color, m_rhs, precision), else PACKED16_PAIRS, PACKED16 or SIMT,
- *            the first that applies. */
+ *            (n_color, m_rhs, precision), else MMA_LINK, PACKED16_PAIRS, PACKED16 or
+ *            SIMT, the first that applies. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2
@@ -322,6 +341,7 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
 #define QCU_HOP_PACKED16_PAIRS 7
 #define QCU_HOP_MMA16 8
 #define QCU_HOP_MMA_LINK 9
+#define QCU_HOP_MMA_LINK_DIRECT 10
 int qcuSetHopKernel(int kind);
 int qcuGetHopKernel(void);
 

@@ -24,8 +24,9 @@ SUCCESS, ERR_INVALID, ERR_STATE, ERR_CUDA, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR
 
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_PRECOND, SOLVER_CGNR = 0, 1, 2, 3, 4
 (HOP_AUTO, HOP_SIMT, HOP_TENSOR, HOP_SIMT_CS, HOP_PACKED16, HOP_PACKED16_ACC16, HOP_PACKED16_STAGED,
- HOP_PACKED16_PAIRS, HOP_MMA16, HOP_MMA_LINK) = range(10)
+ HOP_PACKED16_PAIRS, HOP_MMA16, HOP_MMA_LINK, HOP_MMA_LINK_DIRECT) = range(11)
 PEAK_DFMA, PEAK_FFMA, PEAK_DMMA, PEAK_HMMA, PEAK_BMMA = 1, 2, 3, 4, 5
+HOP_FORM_PLAIN, HOP_FORM_XPAY, HOP_FORM_SCHUR_R0, HOP_FORM_SCHUR_TS, HOP_FORM_SCHUR, HOP_FORM_RESID = range(6)
 MAX_RHS = 64
 
 
@@ -117,6 +118,7 @@ _SIGNATURES = {
     "qcuDslashMrhsXpay": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _i, _i, _d, _i, _vp]),
     "qcuDslashMrhsContext": (_i, [_vp, _vp, _i, _i, _i, _vp]),
     "qcuDslashMrhsContextActive": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp]),
+    "qcuDslashMrhsContextForm": (_i, [_vp, _vp, _vp, _vp, _d, _i, _i, _i, _vp, _vp]),
     "qcuSchurMrhs": (_i, [_vp, _vp, _vp, _vp, _d, _ip, _i, _i, _d, _i, _vp]),
     "qcuGatherMrhs": (_i, [_vp, _i, ctypes.POINTER(_vp), _i, _i64, _i, _i, _vp]),
     "qcuScatterMrhs": (_i, [ctypes.POINTER(_vp), _i, _vp, _i, _i64, _i, _i, _vp]),

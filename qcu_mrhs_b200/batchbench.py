@@ -1,7 +1,7 @@
 """Batched uneven solves: many independent SU(3) systems through qcuInvertBatch vs the
 same systems solved one after another through the qcu.h path (qcuInvert).
 
-  python -m qcu_mrhs_b200.batchbench [--systems 64] [--solver mixed|fp64] [--seed 4]
+  python -m qcu_mrhs_b200.batchbench [--systems 64] [--solver mixed|fp64] [--seed 4] [--out FILE]
 
 Systems are drawn with a seeded generator: lattice from {8^4, 12^4, 16^3 x 32}, m_rhs
 uniform in 1..16, kappa uniform in [0.10, 0.124], smoothed links U = exp(i eps H) with
@@ -124,7 +124,9 @@ def main():
     ap.add_argument("--solver", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--methods", nargs="+", default=["device_loop", "host_loop", "loop"])
+    ap.add_argument("--out", default=None, help="also write every line as one JSON document")
     args = ap.parse_args()
+    lines = []
     import qcu_mrhs_b200 as q
     specs = draw(args.systems, args.seed)
     dev = make_device_fields(specs)
@@ -139,13 +141,19 @@ def main():
         else:
             flags = (q.BATCH_DEVICE_LOOP if method == "device_loop" else q.BATCH_HOST_LOOP) | q.BATCH_KEEP_CONTEXTS
             wall, lat, res, its = run_batch(q, specs, dev, opts, flags)
-        print(json.dumps({
+        line = {
             "method": method, "contexts": "kept from the warm-up call" if method != "loop" else "qcu.h context per system", "solver": args.solver, "systems": len(specs), "rhs": n_rhs,
             "wall_s": wall, "systems_per_s": len(specs) / wall, "rhs_per_s": n_rhs / wall,
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "true_residual_max": res, "iterations_min_max": [min(its), max(its)],
             "lattices": {str(Lx): sum(1 for s in specs if s["L"] == Lx) for Lx in LATTICES},
-        }), flush=True)
+        }
+        lines.append(line)
+        print(json.dumps(line), flush=True)
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump({"systems": len(specs), "seed": args.seed, "solver": args.solver, "rhs": n_rhs,
+                       "results": lines}, f, indent=1)
 
 
     q.lib().qcuBatchRelease()

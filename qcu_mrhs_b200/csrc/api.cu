@@ -525,9 +525,11 @@ int qcuDslashMrhsXpay(void* out, const void* in, const void* gauge, const void* 
                       EPI_XPAY);
 }
 
-// the context's hop (caller holds the API lock)
+// the context's hop (caller holds the API lock); epi selects the fused epilogue (x, r0 and a
+// are its operands, red the [nval][m] double2 output of its reduction or null for scratch)
 static int context_hop(void* out, const void* in, int parity, int dagger, int precision, const int* active,
-                       void* stream) {
+                       void* stream, int epi = EPI_PLAIN, const void* x = nullptr, const void* r0 = nullptr,
+                       double a = 0.0, void* red = nullptr) {
     int rc = require_ctx();
     if (rc) return rc;
     Context& c = *g_ctx;
@@ -556,7 +558,21 @@ static int context_hop(void* out, const void* in, int parity, int dagger, int pr
     p.parity = parity;
     p.t_sign = c.opts.t_boundary;
     p.active = active;
-    return hop_launch(p, c.nc, precision, dagger != 0, EPI_PLAIN, st);
+    p.x = x;
+    p.r0 = r0;
+    p.a = a;
+    if (epi == EPI_SCHUR_R0 || epi == EPI_SCHUR_TS || epi == EPI_RESID) {
+        // the reduction's scratch is the context's, used on its stream: order the caller's
+        // stream after it and the context's stream after this launch
+        p.red = RedArgs{c.ws.partials, c.ws.counter, red ? static_cast<double2*>(red) : c.ws.result, nullptr,
+                        nullptr, FIN_NONE};
+    }
+    int rc2 = hop_launch(p, c.nc, precision, dagger != 0, epi, st);
+    if (rc2 == QCU_SUCCESS && p.red.partials) {
+        QCUB_CUDA_CHECK(cudaEventRecord(c.ev_in, st));
+        QCUB_CUDA_CHECK(cudaStreamWaitEvent(c.stream, c.ev_in, 0));
+    }
+    return rc2;
 }
 
 int qcuDslashMrhsContext(void* out, const void* in, int parity, int dagger, int precision, void* stream) {
@@ -569,6 +585,22 @@ int qcuDslashMrhsContextActive(void* out, const void* in, int parity, int dagger
     QCUB_API_BEGIN
     if (!active) return set_error(QCU_ERR_INVALID, "null activity flags");
     return context_hop(out, in, parity, dagger, precision, active, stream);
+}
+
+static_assert(QCU_HOP_FORM_PLAIN == EPI_PLAIN && QCU_HOP_FORM_XPAY == EPI_XPAY &&
+                  QCU_HOP_FORM_SCHUR_R0 == EPI_SCHUR_R0 && QCU_HOP_FORM_SCHUR_TS == EPI_SCHUR_TS &&
+                  QCU_HOP_FORM_SCHUR == EPI_SCHUR && QCU_HOP_FORM_RESID == EPI_RESID,
+              "hop form codes are the epilogue codes");
+
+int qcuDslashMrhsContextForm(void* out, const void* in, const void* x, const void* r0, double a, int form,
+                             int parity, int precision, void* red, void* stream) {
+    QCUB_API_BEGIN
+    if (form < QCU_HOP_FORM_PLAIN || form > QCU_HOP_FORM_RESID)
+        return set_error(QCU_ERR_INVALID, "hop form %d", form);
+    if (form != QCU_HOP_FORM_PLAIN && !x) return set_error(QCU_ERR_INVALID, "hop form %d needs x", form);
+    if ((form == QCU_HOP_FORM_SCHUR_R0 || form == QCU_HOP_FORM_RESID) && !r0)
+        return set_error(QCU_ERR_INVALID, "hop form %d needs r0", form);
+    return context_hop(out, in, parity, 0, precision, nullptr, stream, form, x, r0, a, red);
 }
 
 int qcuSchurMrhs(void* out, const void* in, void* tmp, const void* gauge, double kappa, const int L[4],
@@ -736,7 +768,7 @@ int qcuDslashMrhsSiteBlocked(void* out, const void* in, const void* gauge, const
 
 int qcuSetHopKernel(int kind) {
     clear_error();
-    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_MMA_LINK)
+    if (kind < QCU_HOP_AUTO || kind > QCU_HOP_MMA_LINK_DIRECT)
         return set_error(QCU_ERR_INVALID, "hop kernel kind %d", kind);
     set_hop_kind(kind);
     return QCU_SUCCESS;

@@ -687,9 +687,9 @@ int launch_mmal_t(const HopParams& p, bool dagger, int epi, int nchunk, cudaStre
 inline bool lalign16(const void* ptr) { return reinterpret_cast<uintptr_t>(ptr) % 16 == 0; }
 
 template <typename S, int NC, int NTC>
-int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, cudaStream_t st) {
+int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, bool staged, cudaStream_t st) {
     const bool pre = p.links != nullptr && p.nbr != nullptr;
-    if (pre && nchunk == 1 && p.m == 4 * NTC && lalign16(p.in) && lalign16(p.links) &&
+    if (staged && pre && nchunk == 1 && p.m == 4 * NTC && lalign16(p.in) && lalign16(p.links) &&
         (!p.x || lalign16(p.x)) && (!p.r0 || lalign16(p.r0)))
     {
         return launch_mmal_tma<S, NC, NTC>(p, dagger, epi, st);
@@ -702,25 +702,25 @@ int launch_mmal_f(const HopParams& p, bool dagger, int epi, int nchunk, cudaStre
 }
 
 template <typename S, int NC>
-int launch_mmal_nc(const HopParams& p, bool dagger, int epi, cudaStream_t st) {
+int launch_mmal_nc(const HopParams& p, bool dagger, int epi, bool staged, cudaStream_t st) {
     // groups of 4 RHS, at most 4 groups per work unit; chunks balanced
     const int groups = (p.m + 3) / 4;
     const int nchunk = (groups + 3) / 4;
     const int ntc = (groups + nchunk - 1) / nchunk;
     switch (ntc) {
-        case 1: return launch_mmal_f<S, NC, 1>(p, dagger, epi, nchunk, st);
-        case 2: return launch_mmal_f<S, NC, 2>(p, dagger, epi, nchunk, st);
-        case 3: return launch_mmal_f<S, NC, 3>(p, dagger, epi, nchunk, st);
-        default: return launch_mmal_f<S, NC, 4>(p, dagger, epi, nchunk, st);
+        case 1: return launch_mmal_f<S, NC, 1>(p, dagger, epi, nchunk, staged, st);
+        case 2: return launch_mmal_f<S, NC, 2>(p, dagger, epi, nchunk, staged, st);
+        case 3: return launch_mmal_f<S, NC, 3>(p, dagger, epi, nchunk, staged, st);
+        default: return launch_mmal_f<S, NC, 4>(p, dagger, epi, nchunk, staged, st);
     }
 }
 
 template <typename S>
-int launch_mmal(const HopParams& p, int nc, bool dagger, int epi, cudaStream_t st) {
+int launch_mmal(const HopParams& p, int nc, bool dagger, int epi, bool staged, cudaStream_t st) {
     switch (nc) {
-        case 2: return launch_mmal_nc<S, 2>(p, dagger, epi, st);
-        case 3: return launch_mmal_nc<S, 3>(p, dagger, epi, st);
-        default: return launch_mmal_nc<S, 4>(p, dagger, epi, st);
+        case 2: return launch_mmal_nc<S, 2>(p, dagger, epi, staged, st);
+        case 3: return launch_mmal_nc<S, 3>(p, dagger, epi, staged, st);
+        default: return launch_mmal_nc<S, 4>(p, dagger, epi, staged, st);
     }
 }
 
@@ -773,7 +773,7 @@ bool hop_mmal_supported(int nc, int m, int prec) {
            m <= kMaxRhs;
 }
 
-int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
+int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool staged, cudaStream_t st) {
     if (!hop_mmal_supported(nc, p.m, prec))
         return set_error(QCU_ERR_UNSUPPORTED, "link-operand tensor-core hop: n_color=%d m_rhs=%d precision=%d", nc,
                          p.m, prec);
@@ -785,8 +785,8 @@ int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, 
     if (p.g.vh * 4 * nc * (int64_t)p.m >= ((int64_t)1 << 31) || p.g.vh * 8 * nc * nc >= ((int64_t)1 << 31))
         return set_error(QCU_ERR_UNSUPPORTED, "link-operand tensor-core hop: field beyond 2^31 complex");
     if (nc >= 5) return hop_mmal_big_launch(p, nc, prec, dagger, epi, st);
-    if (prec == QCU_PRECISION_HALF) return launch_mmal<__half>(p, nc, dagger, epi, st);
-    return launch_mmal<__nv_bfloat16>(p, nc, dagger, epi, st);
+    if (prec == QCU_PRECISION_HALF) return launch_mmal<__half>(p, nc, dagger, epi, staged, st);
+    return launch_mmal<__nv_bfloat16>(p, nc, dagger, epi, staged, st);
 }
 
 }  // namespace qcub

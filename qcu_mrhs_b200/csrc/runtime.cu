@@ -130,7 +130,7 @@ int hop16_pairs_launch(const HopParams& p, int nc, int prec, bool dagger, int ep
 bool hop_mma16_supported(int nc, int m, int prec);
 int hop_mma16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
 bool hop_mmal_supported(int nc, int m, int prec);
-int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st);
+int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool staged, cudaStream_t st);
 int hop16_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool acc16, bool staged,
                  cudaStream_t st);
 
@@ -153,7 +153,7 @@ bool hop_reads_tables(int nc, int m, int prec) {
     if (prec != QCU_PRECISION_HALF && prec != QCU_PRECISION_BF16) return false;
     int kind = g_hop_kind;
     if (kind == QCU_HOP_AUTO) kind = auto_hop_kind(nc, m, prec);
-    return kind == QCU_HOP_MMA_LINK && hop_mmal_supported(nc, m, prec);
+    return (kind == QCU_HOP_MMA_LINK || kind == QCU_HOP_MMA_LINK_DIRECT) && hop_mmal_supported(nc, m, prec);
 }
 
 int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaStream_t st) {
@@ -169,8 +169,8 @@ int hop_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, cudaS
         return hop_tc_launch(p, nc, prec, dagger, epi, st);
     if (kind == QCU_HOP_MMA16 && hop_mma16_supported(nc, p.m, prec))
         return hop_mma16_launch(p, nc, prec, dagger, epi, st);
-    if (kind == QCU_HOP_MMA_LINK && hop_mmal_supported(nc, p.m, prec))
-        return hop_mmal_launch(p, nc, prec, dagger, epi, st);
+    if ((kind == QCU_HOP_MMA_LINK || kind == QCU_HOP_MMA_LINK_DIRECT) && hop_mmal_supported(nc, p.m, prec))
+        return hop_mmal_launch(p, nc, prec, dagger, epi, kind == QCU_HOP_MMA_LINK, st);
     if (kind == QCU_HOP_PACKED16_PAIRS && hop16_pairs_supported(nc, p.m, prec))
         return hop16_pairs_launch(p, nc, prec, dagger, epi, st);
     if ((kind == QCU_HOP_PACKED16 || kind == QCU_HOP_PACKED16_ACC16 || kind == QCU_HOP_PACKED16_STAGED ||

@@ -123,8 +123,11 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
     const int saved = hop_kind();
     // PACKED16_ACC16 is not a candidate: it trades accuracy for speed, so only an explicit
     // request selects it.  Nor is MMA16 (the link-operand kernel supersedes it).
-    int kinds[6] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
-                    QCU_HOP_MMA_LINK};
+    // MMA_LINK and MMA_LINK_DIRECT are the same kernel family with and without the
+    // shared-memory staging (staging pays on lattices far larger than L2; the direct loads
+    // win where the fields stay in L2)
+    int kinds[7] = {QCU_HOP_SIMT, QCU_HOP_SIMT_CS, QCU_HOP_TENSOR, QCU_HOP_PACKED16, QCU_HOP_PACKED16_PAIRS,
+                    QCU_HOP_MMA_LINK, QCU_HOP_MMA_LINK_DIRECT};
     int best = QCU_HOP_SIMT;
     float best_ms = 1e30f;
     for (int kind : kinds) {
@@ -133,6 +136,9 @@ int tune_hop(const int L[4], int nc, int m, int prec, cudaStream_t st, double* b
         if (kind == QCU_HOP_PACKED16 && !hop16_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_PACKED16_PAIRS && !hop16_pairs_supported(nc, m, prec)) continue;
         if (kind == QCU_HOP_MMA_LINK && !hop_mmal_supported(nc, m, prec)) continue;
+        // the direct form differs only where the staged kernel applies (N <= 4, m = 4..16)
+        if (kind == QCU_HOP_MMA_LINK_DIRECT && (!hop_mmal_supported(nc, m, prec) || nc > 4 || m > 16 || m % 4))
+            continue;
         set_hop_kind(kind);
         const bool tables = hop_reads_tables(nc, m, prec);
         if (tables && !links) {

@@ -16,7 +16,7 @@ import json
 
 PRECS = {"f64": 2, "f32": 1, "f16": 0, "bf16": 4}
 KERNELS = ["auto", "simt", "tcgen05", "simt_cs", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs",
-           "mma16", "mma_link", "packed16_pairs_blocked"]
+           "mma16", "mma_link", "mma_link_direct", "packed16_pairs_blocked"]
 # the last entry is the two-RHS kernel on the site-blocked layout (qcuDslashMrhsSiteBlocked)
 BLOCKED = KERNELS.index("packed16_pairs_blocked")
 

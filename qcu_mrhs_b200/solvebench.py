@@ -75,12 +75,15 @@ def main():
         for j in range(m):
             lib.pushBackFermions(outs[j].data_ptr(), ins[j].data_ptr())
         lib.qcuInvert(args.max_iter, args.tol)
-        q.check()
+        st = q.status()
+        if st not in (q.SUCCESS, q.ERR_NOT_CONVERGED):   # a capped --max-iter is a valid run
+            q.check(st)
         s = q.solve_stats()
         print(json.dumps({"repeat": r, "L": list(L), "nc": nc, "m": m, "solver": args.solver,
                           "sloppy": args.sloppy if args.solver == "mixed" else None,
                           "iterations": s.iterations, "reliable_updates": s.reliable_updates,
-                          "solve_seconds": s.solve_seconds, "true_residual_max": max(s.true_residual[:m])}),
+                          "solve_seconds": s.solve_seconds, "true_residual_max": max(s.true_residual[:m]),
+                          "converged": st == q.SUCCESS}),
               flush=True)
     lib.qcuSetHopKernel(0)
     lib.finalizeQcu()

@@ -48,6 +48,8 @@ def applicable(kernel, nc, m, prec):
         return low and 2 <= nc <= 4 and m >= 2
     if kernel == "mma_link":
         return low and 2 <= nc <= 8
+    if kernel == "mma_link_direct":   # differs from mma_link only where that one stages
+        return low and 2 <= nc <= 4 and m <= 16 and m % 4 == 0
     return False
 
 
@@ -101,7 +103,8 @@ def main():
     ap.add_argument("--nc", type=int, nargs="+", default=[2, 3, 4, 5, 6, 7, 8])
     ap.add_argument("--m", type=int, nargs="+", default=[8, 16, 32])
     ap.add_argument("--prec", nargs="+", default=["f64", "f32", "f16", "bf16"])
-    ap.add_argument("--kernels", nargs="+", default=["simt", "simt_cs", "tcgen05", "packed16", "mma_link"])
+    ap.add_argument("--kernels", nargs="+", default=["simt", "simt_cs", "tcgen05", "packed16", "mma_link",
+                                                      "mma_link_direct"])
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--out", default=None, help="also write every line as one JSON document")
     ap.add_argument("--merge-ncu", default=None, help="ncu CSV of a --kernels mma_link --reps 1 sweep")

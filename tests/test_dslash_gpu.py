@@ -98,9 +98,9 @@ def _acc16_factor(kind, prec):
 
 
 LOWP_KERNELS = [q.HOP_SIMT, q.HOP_SIMT_CS, q.HOP_TENSOR, q.HOP_PACKED16, q.HOP_PACKED16_ACC16,
-                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS, q.HOP_MMA16, q.HOP_MMA_LINK]
+                q.HOP_PACKED16_STAGED, q.HOP_PACKED16_PAIRS, q.HOP_MMA16, q.HOP_MMA_LINK, q.HOP_MMA_LINK_DIRECT]
 LOWP_IDS = ["simt", "simt_cs", "tcgen05", "packed16", "packed16_acc16", "packed16_staged", "packed16_pairs", "mma16",
-            "mma_link"]
+            "mma_link", "mma_link_direct"]
 
 
 @pytest.mark.parametrize("hop_kernel", LOWP_KERNELS, indirect=True, ids=LOWP_IDS)
