@@ -51,7 +51,10 @@ CHECK_INTERVAL = 16
 # DRAM bytes of one hop launch on this workload (dram__bytes.sum.per_second x
 # gpu__time_duration from one ncu capture of the kernel at this size, plain epilogue);
 # keyed by (storage precision, kernel)
-MEASURED_TRAFFIC = {("f16", "packed16_pairs"): 490.7e6, ("f16", "packed16"): 530.2e6, ("f16", "simt"): 610.6e6}
+# DRAM bytes (read + write) per launch of the plain hop on this workload, from one ncu capture
+# of dram__bytes_read.sum + dram__bytes_write.sum (mean of 3 launches)
+MEASURED_TRAFFIC = {("f16", "packed16_pairs"): 490.7e6, ("f16", "packed16"): 530.2e6, ("f16", "simt"): 610.6e6,
+                    ("f16", "mma_link"): 651.0e6, ("bf16", "mma_link"): 647.6e6, ("f64", "simt"): 2255.7e6}
 # arithmetic of each 16-bit hop kernel
 DTYPE_DETAIL = {
     "mma_link_direct": "FP16 storage; spin projection in FP16 (one rounding), link products and the sum of the 8 "

@@ -256,30 +256,6 @@ __device__ __forceinline__ void hop_store(const typename St<S>::A2 (&acc)[4][NC]
         }
 }
 
-// L2 prefetch of a site's epilogue operands (x and, for the forms that read it, r0), issued
-// one site ahead: thread RHS r takes the spin-colour rows r, r + m, ... of the site
-// block (each row m complex words, all RHS), one prefetch per 128-byte line, so the
-// epilogue's loads hit L2 instead of waiting on DRAM after the hop arithmetic.
-template <int NC, typename S, int EPI>
-__device__ __forceinline__ void prefetch_epilogue(const HopParams& p, int64_t site_base, int rhs) {
-    using S2 = typename St<S>::S2;
-    const int m = p.m;
-    const int rowb = m * (int)sizeof(S2);
-    constexpr bool R0 = EPI == EPI_SCHUR_R0 || EPI == EPI_RESID;
-    for (int row = rhs; row < kNs * NC; row += m) {
-        const char* xr = reinterpret_cast<const char*>(static_cast<const S2*>(p.x) + site_base + (int64_t)row * m);
-        const char* rr = R0 ? reinterpret_cast<const char*>(static_cast<const S2*>(p.r0) + site_base +
-                                                            (int64_t)row * m)
-                            : nullptr;
-        for (int o = 0; o < rowb; o += 128) {
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(xr + o));
-            if (R0) asm volatile("prefetch.global.L2 [%0];" ::"l"(rr + o));
-        }
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(xr + rowb - 1));
-        if (R0) asm volatile("prefetch.global.L2 [%0];" ::"l"(rr + rowb - 1));
-    }
-}
-
 // Minimum resident blocks per SM requested from the register allocator: FP64 at small N
 // otherwise takes ~190 registers (one block per SM, latency-bound); capping it at 128
 // doubles the warps in flight.  Large N keeps the compiler's choice (accumulators dominate).
@@ -308,17 +284,11 @@ __global__ void __launch_bounds__(kRedThreads, HopMinBlocks<NC, S>::value) hop_k
     // walks sites without dividing
     const int64_t site_stride = stride / m;
     (void)total;
-    const int64_t site0 = ((int64_t)blockIdx.x * blockDim.x) / m + threadIdx.x / m;
-    if constexpr (EPI != EPI_PLAIN)
-        if (site0 < p.g.vh) prefetch_epilogue<NC, S, EPI>(p, site0 * site_len, rhs);
-    for (int64_t site = site0; site < p.g.vh; site += site_stride) {
+    for (int64_t site = ((int64_t)blockIdx.x * blockDim.x) / m + threadIdx.x / m; site < p.g.vh;
+         site += site_stride) {
         A2 acc[4][NC];
         hop_site<NC, S, DAG>(acc, p, site, rhs);
         hop_store<NC, S, EPI, NV>(acc, p, site * site_len + rhs, red);
-        // the next site's epilogue operands, requested a whole site ahead (the registers of
-        // this site's hop are free again here)
-        if constexpr (EPI != EPI_PLAIN)
-            if (site + site_stride < p.g.vh) prefetch_epilogue<NC, S, EPI>(p, (site + site_stride) * site_len, rhs);
     }
     if constexpr (NV > 0) {
         double2 rv[NV];
