@@ -329,8 +329,8 @@ int qcuDslashMrhsSiteBlocked(void *out, const void *in, const void *gauge, const
  *   MMA_LINK_DIRECT  the same kernels without the shared-memory staging (fragment words
  *            loaded straight from global memory): faster where the fields stay in L2;
  *   AUTO     the choice recorded by qcuTuneHop (or loaded from the tuning cache) for
- *            (n_color, m_rhs, precision), else MMA_LINK, PACKED16_PAIRS, PACKED16 or
- *            SIMT, the first that applies. */
+ *            (n_color, m_rhs, precision), else MMA_LINK (n_color >= 5 or m_rhs <= 16),
+ *            PACKED16_PAIRS, PACKED16 or SIMT, the first that applies. */
 #define QCU_HOP_AUTO 0
 #define QCU_HOP_SIMT 1
 #define QCU_HOP_TENSOR 2

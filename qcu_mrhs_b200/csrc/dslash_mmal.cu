@@ -14,13 +14,13 @@ template <typename S, int MU, int SF, int NTC, bool EXACT>
 __device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __restrict__ pf,
                                          const uint32_t* __restrict__ qf, const uint32_t* __restrict__ pb,
                                          const uint32_t* __restrict__ qb, const uint32_t (&A)[4], uint32_t lmf,
-                                         uint32_t lmb, int rb0, int q, int m, uint32_t gmask) {
+                                         uint32_t lmb, int rb0, int q, int m) {
     using M = LMma<S>;
     constexpr int SB = -SF;
     uint32_t w[NTC][4];
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!((gmask >> n) & 1u)) continue;   // warp-uniform: absent or inactive group
+        if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
         int d = 4 * n;
         if (!EXACT) d += min(0, m - 1 - (rb0 + 4 * n + q));   // last partial group: clamp the RHS
         w[n][0] = __ldg(pf + d);
@@ -30,7 +30,7 @@ __device__ __forceinline__ void mmal_dir(float (&Q)[NTC][4], const uint32_t* __r
     }
 #pragma unroll
     for (int n = 0; n < NTC; ++n) {
-        if (!((gmask >> n) & 1u)) continue;
+        if (!EXACT && rb0 + 4 * n >= m) break;
         const uint32_t hf = lproject<S, MU, SF>(w[n][0], w[n][1], lmf);
         const uint32_t hb = lproject<S, MU, SB>(w[n][2], w[n][3], lmb);
         M::mma(Q[n], A, hf, hb, Q[n][0], Q[n][1], Q[n][2], Q[n][3]);
@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
     const uint32_t site_stride = (uint32_t)(nw / nchunk);
     const uint32_t site0 = gw < (int64_t)site_stride * nchunk ? (uint32_t)(gw / nchunk) : vh;
     const int rb0 = chunk * NTC * 4;
+    // groups with a live RHS (per-RHS activity flags); the others are loaded and computed
+    // like the rest (no per-group branches between the loads) but not stored
     const uint32_t gmask = active_groups<NTC>(p.active, rb0, m);
     const uint32_t* __restrict__ inA = in + rb0 + (hh * NC + ct) * m;
     const uint32_t* __restrict__ inB01 = in + rb0 + ((3 - hh) * NC + ct) * m;
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
 #pragma unroll
             for (int n = 0; n < NTC; ++n) {
                 xw[n][0] = xw[n][1] = yw[n][0] = yw[n][1] = 0u;
-                if (!((gmask >> n) & 1u)) continue;
+                if (!EXACT && rb0 + 4 * n >= m) break;
                 if (sok && (EXACT || rb0 + 4 * n + t < m)) {
                     const size_t o = sbase + os + 4 * n;
                     xw[n][0] = __ldg(xv + o);
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         // x - y (the y projector's spin-3 phase is minus its diff-row phase)
         mmal_a(A, wf[1], wb[1], okm, ph1.sel, ph1.mf, ph1.mb);
         mmal_dir<S, 1, SF, NTC, EXACT>(Qxy, inA + (size_t)nb2 * SW, inB01 + (size_t)nb2 * SW, inA + (size_t)nb3 * SW,
-                                       inB01 + (size_t)nb3 * SW, A, m1f, m1b, rb0, q, m, gmask);
+                                       inB01 + (size_t)nb3 * SW, A, m1f, m1b, rb0, q, m);
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
             Qxy[n][0] *= fl;
@@ -191,12 +193,12 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         }
         mmal_a(A, wf[0], wb[0], okm, ph0.sel, ph0.mf, ph0.mb);
         mmal_dir<S, 0, SF, NTC, EXACT>(Qxy, inA + (size_t)nb0 * SW, inB01 + (size_t)nb0 * SW, inA + (size_t)nb1 * SW,
-                                       inB01 + (size_t)nb1 * SW, A, 0u, 0u, rb0, q, m, gmask);
+                                       inB01 + (size_t)nb1 * SW, A, 0u, 0u, rb0, q, m);
         // z, then spin 3 (diff column h1, registers 1 and 3) negated, then t (boundary sign
         // folded into the links)
         mmal_a(A, wf[2], wb[2], okm, ph2.sel, ph2.mf, ph2.mb);
         mmal_dir<S, 2, SF, NTC, EXACT>(Qzt, inA + (size_t)nb4 * SW, inB23 + (size_t)nb4 * SW, inA + (size_t)nb5 * SW,
-                                       inB23 + (size_t)nb5 * SW, A, m2f, m2b, rb0, q, m, gmask);
+                                       inB23 + (size_t)nb5 * SW, A, m2f, m2b, rb0, q, m);
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
             Qzt[n][1] *= fl;
@@ -204,11 +206,11 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
         }
         mmal_a(A, wf[3], wb[3], okm, ph3.sel, ph3.mf, ph3.mb);
         mmal_dir<S, 3, SF, NTC, EXACT>(Qzt, inA + (size_t)nb6 * SW, inB23 + (size_t)nb6 * SW, inA + (size_t)nb7 * SW,
-                                       inB23 + (size_t)nb7 * SW, A, 0u, 0u, rb0, q, m, gmask);
+                                       inB23 + (size_t)nb7 * SW, A, 0u, 0u, rb0, q, m);
 
 #pragma unroll
         for (int n = 0; n < NTC; ++n) {
-            if (!((gmask >> n) & 1u)) continue;   // warp-uniform
+            if (!EXACT && rb0 + 4 * n >= m) break;   // warp-uniform
             const bool rok = sok && (EXACT || rb0 + 4 * n + t < m);
             const size_t o = sbase + os + 4 * n;
             // the lane's two spins (2 cls, 2 cls + 1) of (colour g % 4, RHS t): sum lanes take
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
             ov[0].y = Qzt[n][2] + (cls ? Qxy[n][3] : Qxy[n][2]);
             ov[1].x = Qzt[n][1] + (cls ? Qxy[n][0] : Qxy[n][1]);
             ov[1].y = Qzt[n][3] + (cls ? Qxy[n][2] : Qxy[n][3]);
-            if (!rok) continue;
+            if (!rok || !((gmask >> n) & 1u)) continue;
             if constexpr (EPI == EPI_PLAIN) {
                 out[o] = M::pack(ov[0].x, ov[0].y);
                 out[o + osn] = M::pack(ov[1].x, ov[1].y);
@@ -257,7 +259,6 @@ __global__ void __launch_bounds__(kLThreads, LMinBlocks<EPI>::value) hop_mmal_ke
             }
         }
     }
-
     if constexpr (NV > 0) {
         // lanes (g, t) hold RHS rb0 + 4n + t: sum over g (fixed butterfly), then over the
         // block's warps of the same chunk in order, then the common grid stage

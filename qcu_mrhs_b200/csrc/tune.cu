@@ -62,10 +62,11 @@ int auto_hop_kind(int nc, int m, int prec) {
         auto it = g_tuned.find(std::make_tuple(current_device(), nc, m, prec));
         if (it != g_tuned.end()) return it->second;
     }
-    // measured on B200 (16^4 and 24^3x48, N = 3..8, m = 8..32): packed 16-bit arithmetic
-    // wins for FP16/BF16 storage wherever it applies (two RHS per thread where that is
-    // specialised), the per-(site, RHS) SIMT kernel everywhere else
-    if (hop_mmal_supported(nc, m, prec)) return QCU_HOP_MMA_LINK;
+    // measured on B200 (16^4 and 24^3x48, N = 2..8, m = 8..32): for FP16/BF16 storage the
+    // link-operand tensor-core hop wins at N >= 5 and, for N <= 4, up to 16 RHS (where it
+    // stages its blocks in shared memory); beyond that the two-RHS packed kernel (24^3x48,
+    // m = 32: 838 us against 1144 us), else packed 16-bit arithmetic, else SIMT
+    if (hop_mmal_supported(nc, m, prec) && (nc >= 5 || m <= 16)) return QCU_HOP_MMA_LINK;
     if (hop16_pairs_supported(nc, m, prec)) return QCU_HOP_PACKED16_PAIRS;
     if (hop16_supported(nc, m, prec)) return QCU_HOP_PACKED16;
     return QCU_HOP_SIMT;
