@@ -360,6 +360,14 @@ int qcuGetAutoHop(int n_color, int m_rhs, int precision);
  * invalid); synchronises the device.  clear != 0 resets the flag. */
 int qcuGetKernelError(int clear);
 
+/* Self-test of the bounded waits of the staged tensor-core hop on the current context
+ * (n_color <= 4, m_rhs = 4, 8, 12 or 16): one FP16 hop launch whose shared-memory stages
+ * are armed but never filled, so that every wait gives up after limit_cycles clock cycles
+ * and the kernel ends with the device error flag set instead of hanging.  *timed_out = 1
+ * when the flag was set (the expected outcome); the flag is cleared again and the context
+ * stays usable. */
+int qcuHopWaitSelfTest(long long limit_cycles, int *timed_out);
+
 /* Device synchronisation helper for bindings that have no CUDA runtime of their own. */
 int qcuDeviceSynchronize(void);
 

@@ -147,6 +147,7 @@ _SIGNATURES = {
     "qcuGetAutoHop": (_i, [_i, _i, _i]),
     "qcuDeviceSynchronize": (_i, []),
     "qcuPeakRate": (_i, [_i, _i, ctypes.POINTER(_d), _vp]),
+    "qcuHopWaitSelfTest": (_i, [ctypes.c_longlong, ctypes.POINTER(_i)]),
     "qcuPrecondCreate": (_i, [ctypes.POINTER(_vp), _ip, _i, _i, _i, _i, _d]),
     "qcuPrecondDestroy": (_i, [_vp]),
     "qcuPrecondNumWeights": (_i64, [_vp]),

@@ -19,6 +19,8 @@ int last_status();
 int hop_kind();
 void set_hop_kind(int k);
 int* device_error_flag();
+bool hop_mmal_supported(int nc, int m, int prec);
+int hop_mmal_launch(const HopParams& p, int nc, int prec, bool dagger, int epi, bool staged, cudaStream_t st);
 const char* last_message();
 
 int DevBuf::ensure(size_t nbytes) {
@@ -785,6 +787,54 @@ int qcuGetKernelError(int clear) {
     QCUB_CUDA_CHECK(cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (clear) QCUB_CUDA_CHECK(cudaMemset(flag, 0, sizeof(int)));
     return h;
+}
+
+int qcuHopWaitSelfTest(long long limit_cycles, int* timed_out) {
+    QCUB_API_BEGIN
+    if (!timed_out || limit_cycles < 1) return set_error(QCU_ERR_INVALID, "qcuHopWaitSelfTest: arguments");
+    int rc = require_ctx();
+    if (rc) return rc;
+    Context& c = *g_ctx;
+    if ((rc = require_dslash(c))) return rc;
+    const int prec = QCU_PRECISION_HALF;
+    if (!hop_mmal_supported(c.nc, c.m, prec) || c.nc > 4 || c.m > 16 || c.m % 4)
+        return set_error(QCU_ERR_UNSUPPORTED, "qcuHopWaitSelfTest: the staged hop needs n_color <= 4, m_rhs = 4..16");
+    const void* gauge = nullptr;
+    const void* links = nullptr;
+    const uint32_t* nbr = nullptr;
+    if ((rc = c.gauge_in(prec, &gauge))) return rc;
+    if ((rc = c.hop_tables(prec, c.opts.t_boundary, &links, &nbr))) return rc;
+    int* flag = device_error_flag();
+    if (!flag) return set_error(QCU_ERR_CUDA, "device error flag unavailable");
+    void* buf = nullptr;
+    const size_t hb = c.half_bytes(prec);
+    QCUB_CUDA_CHECK(cudaMalloc(&buf, 2 * hb));
+    HopParams p{};
+    p.out = static_cast<char*>(buf) + hb;
+    p.in = buf;
+    p.gauge = gauge;
+    p.links = links;
+    p.nbr = nbr;
+    p.g = c.g;
+    p.m = c.m;
+    p.parity = 0;
+    p.t_sign = c.opts.t_boundary;
+    p.wait_limit = limit_cycles;
+    p.wait_test = 1;
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        rc = hop_mmal_launch(p, c.nc, prec, false, EPI_PLAIN, true, c.stream);
+        if (rc == QCU_SUCCESS) e = cudaStreamSynchronize(c.stream);
+    }
+    int h = 0;
+    if (rc == QCU_SUCCESS && e == cudaSuccess) e = cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (rc == QCU_SUCCESS && e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(int));
+    cudaFree(buf);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(QCU_ERR_CUDA, "qcuHopWaitSelfTest: %s", cudaGetErrorString(e));
+    *timed_out = h != 0;
+    return QCU_SUCCESS;
 }
 
 int qcuDeviceSynchronize(void) {

@@ -54,6 +54,11 @@ struct HopParams {
     // optional per-RHS flags (device int[m]): the tensor-core hop skips every group of 4 RHS
     // whose flags are all 0 (its outputs are then left as they were); null = all active
     const int* active;
+    // bounded waits of the staged tensor-core hop: the limit in clock cycles (0: about a
+    // second), and a self-test mode in which its stages are armed but never filled, so that
+    // every wait runs out and the kernel ends with the device error flag set
+    long long wait_limit;
+    int wait_test;
 };
 
 __device__ __forceinline__ bool skip_launch(const int* done, const int* gate) {

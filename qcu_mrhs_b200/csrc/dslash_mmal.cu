@@ -324,13 +324,13 @@ __device__ __forceinline__ bool lbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait: the clock is read only once the first try has failed (in the common case
-// the copies have landed and the wait costs one try)
-__device__ __forceinline__ bool lbar_wait(uint32_t bar, uint32_t parity) {
+// the copies have landed and the wait costs one try); gives up after `limit` cycles
+__device__ __forceinline__ bool lbar_wait(uint32_t bar, uint32_t parity, long long limit) {
     if (lbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (lbar_try(bar, parity)) return true;
-        if (clock64() - t0 > (1ll << 31)) return false;   // about a second
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -427,7 +427,10 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
     // lanes 0-7 take neighbour nbi, lane 8 the links, lanes 9-10 the epilogue blocks)
     // lane roles of a copy round, fixed for the kernel: source base and per-site stride,
     // destination offset in the stage, bytes; the copy itself is predicated, not branched
-    const bool cp_nb = lane < 8, cp_on = lane < 9 + NX;
+    // (wait self-test: the barrier is armed, no copy is issued, every wait runs out)
+    const bool cp_nb = lane < 8, cp_on = lane < 9 + NX && !p.wait_test;
+    const long long wlim = p.wait_limit > 0 ? p.wait_limit : (1ll << 31);   // about a second
+    const uint32_t cp_flight = p.wait_test ? 0u : 1u;   // 1: a stage's copies are in flight
     const unsigned char* cp_base = lane == 8 ? links + (size_t)parity * vh * (LW * 4)
                                  : (lane == 9 ? xv : (lane == 10 ? yv : in));
     const uint32_t cp_stride = lane == 8 ? LW * 4 : SBY;
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
         uint32_t use = 0;        // uses of each stage so far (bit k = parity of stage k's next wait)
         if (site < vh) {
             issue(0, site, lane < 8 ? __ldg(nbr + (size_t)site * 8 + lane) : 0u);
-            inflight |= 1u;
+            inflight |= cp_flight;
         }
         // neighbour index of the next site, loaded one site ahead
         uint32_t nb_next = (site + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(site + nw) * 8 + lane) : 0u;
@@ -487,10 +490,10 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
             const uint32_t nxt = site + nw;
             if (nxt < vh) {   // the other stage was released by the previous site's __syncwarp
                 issue(k ^ 1, nxt, nb_next);
-                inflight |= 2u >> k;
+                inflight |= cp_flight << (k ^ 1);
                 nb_next = (nxt + nw < vh && lane < 8) ? __ldg(nbr + (size_t)(nxt + nw) * 8 + lane) : 0u;
             }
-            if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) {
+            if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u, wlim)) {
                 ok = false;
                 break;
             }
@@ -582,7 +585,7 @@ __global__ void __launch_bounds__(kTThreads) hop_mmal_tma_kernel(const HopParams
             if (lane == 0) atomicExch(err, 1);
             for (int k = 0; k < kTStages; ++k)
                 if ((inflight >> k) & 1u) {
-                    if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u)) break;
+                    if (!lbar_wait(bar0 + 8 * k, (use >> k) & 1u, wlim)) break;
                 }
         }
         // partial sums back to their groups

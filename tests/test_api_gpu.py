@@ -344,6 +344,39 @@ def test_context_hop_forms(oracle_lib, prec, form):
     assert q.lib().qcuGetKernelError(1) == 0
 
 
+def test_staged_hop_bounded_wait_gives_up_with_an_error(oracle_lib):
+    """The staged tensor-core hop's bounded waits: with its stages armed but never filled
+    (qcuHopWaitSelfTest) every wait gives up after the given cycle count and the kernel ends
+    with the device error flag set, instead of hanging; afterwards the flag is clear and the
+    context's hop still matches the oracle."""
+    L, nc, m, kappa = (8, 4, 4, 8), 3, 12, 0.11
+    gauge, dg = _setup(L, nc, m, kappa, 91)
+    o = q.default_options()
+    o.t_boundary = -1.0
+    q.check(q.lib().qcuSetSolverOptions(ctypes.byref(o)))
+    q.check(q.lib().qcuSetHopKernel(q.HOP_MMA_LINK))
+    timed_out = ctypes.c_int(0)
+    q.check(q.lib().qcuHopWaitSelfTest(1 << 20, ctypes.byref(timed_out)))
+    assert timed_out.value == 1
+    assert q.lib().qcuGetKernelError(1) == 0
+    inp = F.to_mrhs(F.gaussian_fermions(L, nc, m, 92, parities=1)[:, 0])
+    d_in = to_dev(inp, q.HALF)
+    d_out = empty_dev(inp.shape, q.HALF)
+    q.check(q.lib().qcuDslashMrhsContext(d_out.data_ptr(), d_in.data_ptr(), 0, 0, q.HALF, None))
+    sync()
+    ref = oracle_lib.hop(_round(inp, q.HALF), _round(gauge, q.HALF), L, 0, False, -1.0)
+    assert rel_err(from_dev(d_out), ref) <= 2e-3
+    assert q.lib().qcuGetKernelError(1) == 0
+
+
+def test_wait_self_test_rejects_unstaged_shapes():
+    L, nc, m, kappa = (4, 4, 4, 4), 3, 6, 0.11
+    _setup(L, nc, m, kappa, 93)
+    timed_out = ctypes.c_int(0)
+    assert q.lib().qcuHopWaitSelfTest(1 << 20, ctypes.byref(timed_out)) == q.ERR_UNSUPPORTED
+    assert q.lib().qcuHopWaitSelfTest(0, ctypes.byref(timed_out)) == q.ERR_INVALID
+
+
 _LAST = {"error": ""}
 
 
